@@ -1,0 +1,416 @@
+// extern "C" entry points of include/cfdg.h.  Every call converts library
+// failures into a status code and keeps the message for cfdg_last_error().
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "cfdg.h"
+#include "host_mesh.hpp"
+#include "solver.hpp"
+
+struct cfdg_solver {
+    cfdg::Solver* impl;
+    int device;
+};
+struct cfdg_bsr {
+    cudaStream_t stream;
+    cfdg::BsrSystem* impl;
+    int device;
+};
+struct cfdg_host_mesh {
+    cfdg::HostMesh mesh;
+};
+
+namespace cfdg {
+namespace {
+thread_local std::string g_last_error;
+}
+void set_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace cfdg
+
+namespace {
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return CFDG_OK;
+    } catch (const cfdg::Failure& e) {
+        cfdg::set_error(e.msg);
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        cfdg::set_error("host allocation failed");
+        return CFDG_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        cfdg::set_error(e.what());
+        return CFDG_ERR_INVALID;
+    } catch (...) {
+        cfdg::set_error("unknown failure");
+        return CFDG_ERR_INVALID;
+    }
+}
+
+int require_device(int device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        cfdg::set_error("no CUDA device visible");
+        return CFDG_ERR_NODEVICE;
+    }
+    if (device < 0 || device >= count) {
+        cfdg::set_error("device index out of range");
+        return CFDG_ERR_INVALID;
+    }
+    return CFDG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfdg_version(void) { return 10000; }
+
+const char* cfdg_status_string(int status) {
+    switch (status) {
+        case CFDG_OK: return "ok";
+        case CFDG_ERR_INVALID: return "invalid argument";
+        case CFDG_ERR_CUDA: return "CUDA error";
+        case CFDG_ERR_NOMEM: return "out of memory";
+        case CFDG_ERR_SINGULAR: return "singular diagonal block";
+        case CFDG_ERR_NONFINITE: return "non-finite value";
+        case CFDG_ERR_DIVERGED: return "Krylov breakdown";
+        case CFDG_ERR_MESH: return "invalid mesh";
+        case CFDG_ERR_UNSUPPORTED: return "unsupported option";
+        case CFDG_ERR_NODEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* cfdg_last_error(void) { return cfdg::g_last_error.c_str(); }
+
+int cfdg_device_count(int* count_h) {
+    if (!count_h) return CFDG_ERR_INVALID;
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) {
+        cudaGetLastError();
+        c = 0;
+    }
+    *count_h = c;
+    return CFDG_OK;
+}
+
+void cfdg_config_default(cfdg_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    // SolverConfig / SolverParams defaults (solver/compressible/config.hpp:94-136,
+    // linalg/config.hpp:14-26), implicit MUSCL + LSQ as on the hot path.
+    c->viscous = 0;
+    c->turbulence = 0;
+    c->gradient = CFDG_GRAD_LSQ_NODE;
+    c->reconstruction = CFDG_RECON_MUSCL;
+    c->limiter = CFDG_LIM_VENKATAKRISHNAN;
+    c->precision = CFDG_PREC_FP64;
+    c->precond = CFDG_PC_SGS;
+    c->sgs_ordering = CFDG_SGS_COLOR;
+    c->sgs_sweeps = 1;
+    c->lin_max_iterations = 500;
+    c->cfl_ramp_iterations = 0;
+    c->residual_interval = 1;
+    c->gamma = 1.4;
+    c->gas_constant = 287.052874;
+    c->prandtl = 0.71;
+    c->prandtl_turb = 0.9;
+    c->init_rho = 1.225;
+    c->init_p = 101325.0;
+    c->venkat_k = 0.5;
+    c->cfl = 0.4;
+    c->cfl_max = 0.4;
+    c->residual_tolerance = 1.0e-10;
+    c->lin_rel_tol = 1.0e-1;
+    c->lin_abs_tol = 1.0e-15;
+    c->nu_inf_ratio = 3.0;
+    c->max_iterations = 10000;
+}
+
+// ------------------------------------------------------------------ meshes
+int cfdg_mesh_generate(const cfdg_mesh_spec* spec, cfdg_host_mesh** out) {
+    if (!spec || !out) return CFDG_ERR_INVALID;
+    *out = nullptr;
+    return guarded([&] {
+        auto* m = new cfdg_host_mesh();
+        std::string err;
+        const int st = cfdg::generate_mesh(*spec, m->mesh, err);
+        if (st != CFDG_OK) {
+            delete m;
+            throw cfdg::Failure{st, err};
+        }
+        *out = m;
+    });
+}
+
+int cfdg_host_mesh_view(const cfdg_host_mesh* mesh, cfdg_mesh_host* view) {
+    if (!mesh || !view) return CFDG_ERR_INVALID;
+    mesh->mesh.view(*view);
+    return CFDG_OK;
+}
+
+int cfdg_host_mesh_free(cfdg_host_mesh* mesh) {
+    delete mesh;
+    return CFDG_OK;
+}
+
+int cfdg_mesh_compute_geometry(cfdg_host_mesh* mesh) {
+    if (!mesh) return CFDG_ERR_INVALID;
+    return guarded([&] {
+        std::string err;
+        if (!cfdg::compute_geometry(mesh->mesh, err)) throw cfdg::Failure{CFDG_ERR_MESH, err};
+    });
+}
+
+// ------------------------------------------------------------------ solver
+int cfdg_solver_create(int device, const cfdg_mesh_host* mesh, const cfdg_config* cfg, const cfdg_bc_desc* bcs,
+                       int32_t n_bcs, cfdg_solver** out) {
+    if (!mesh || !cfg || !out || (n_bcs > 0 && !bcs) || n_bcs < 0) return CFDG_ERR_INVALID;
+    *out = nullptr;
+    const int dev = require_device(device);
+    if (dev != CFDG_OK) return dev;
+    return guarded([&] {
+        auto* s = new cfdg_solver{nullptr, device};
+        try {
+            s->impl = new cfdg::Solver(device, *mesh, *cfg, bcs, n_bcs);
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+int cfdg_solver_destroy(cfdg_solver* s) {
+    if (!s) return CFDG_OK;
+    const int st = guarded([&] { delete s->impl; });
+    delete s;
+    return st;
+}
+
+#define CFDG_SOLVER_CALL(s, ...)                     \
+    if (!(s) || !(s)->impl) return CFDG_ERR_INVALID; \
+    return guarded([&] { cudaSetDevice((s)->device); __VA_ARGS__; })
+
+int cfdg_solver_init_fields(cfdg_solver* s) { CFDG_SOLVER_CALL(s, s->impl->init_fields()); }
+
+int cfdg_solver_set_state(cfdg_solver* s, const double* u_h, int64_t ld) {
+    if (!u_h) return CFDG_ERR_INVALID;
+    CFDG_SOLVER_CALL(s, s->impl->set_state_host(u_h, ld));
+}
+
+int cfdg_solver_get_field(cfdg_solver* s, int32_t field, double* out_h, int64_t count) {
+    if (!out_h) return CFDG_ERR_INVALID;
+    CFDG_SOLVER_CALL(s, s->impl->get_field(field, out_h, count));
+}
+
+int cfdg_solver_sizes(const cfdg_solver* s, int64_t* sizes_h) {
+    if (!s || !s->impl || !sizes_h) return CFDG_ERR_INVALID;
+    s->impl->sizes(sizes_h);
+    return CFDG_OK;
+}
+
+int cfdg_evaluate_residual(cfdg_solver* s) {
+    CFDG_SOLVER_CALL(s, s->impl->evaluate_residual(); cfdg::cuda_check(cudaStreamSynchronize(s->impl->stream()), "sync"));
+}
+
+int cfdg_solver_stage(cfdg_solver* s, int32_t stage) {
+    CFDG_SOLVER_CALL(s, s->impl->stage(stage); cfdg::cuda_check(cudaStreamSynchronize(s->impl->stream()), "sync"));
+}
+
+int cfdg_compute_dt(cfdg_solver* s, double cfl) {
+    CFDG_SOLVER_CALL(s, s->impl->compute_dt(cfl); cfdg::cuda_check(cudaStreamSynchronize(s->impl->stream()), "sync"));
+}
+
+int cfdg_assemble_jacobian(cfdg_solver* s) {
+    CFDG_SOLVER_CALL(s, s->impl->assemble_jacobian(); cfdg::cuda_check(cudaStreamSynchronize(s->impl->stream()), "sync"));
+}
+
+int cfdg_linear_solve(cfdg_solver* s, cfdg_krylov_result* out_h) {
+    CFDG_SOLVER_CALL(s, {
+        const cfdg_krylov_result r = s->impl->linear_solve();
+        if (out_h) *out_h = r;
+    });
+}
+
+int cfdg_newton_step(cfdg_solver* s, double cfl, cfdg_step_result* out_h) {
+    CFDG_SOLVER_CALL(s, {
+        const cfdg_step_result r = s->impl->newton_step(cfl);
+        if (out_h) *out_h = r;
+    });
+}
+
+int cfdg_residual_norms(cfdg_solver* s, double* l2_h) {
+    if (!l2_h) return CFDG_ERR_INVALID;
+    CFDG_SOLVER_CALL(s, s->impl->residual_norms(l2_h));
+}
+
+int cfdg_run_steady(cfdg_solver* s, cfdg_run_result* out_h) {
+    CFDG_SOLVER_CALL(s, {
+        const cfdg_run_result r = s->impl->run_steady();
+        if (out_h) *out_h = r;
+    });
+}
+
+void* cfdg_solver_stream(cfdg_solver* s) { return (s && s->impl) ? static_cast<void*>(s->impl->stream()) : nullptr; }
+
+int64_t cfdg_solver_launch_count(const cfdg_solver* s) { return (s && s->impl) ? s->impl->launches() : -1; }
+
+int cfdg_solver_profile(cfdg_solver* s, int32_t enable) {
+    CFDG_SOLVER_CALL(s, {
+        cfdg::cuda_check(cudaStreamSynchronize(s->impl->stream()), "sync");
+        s->impl->profiler().collect();
+        s->impl->profiler().enable(enable != 0);
+    });
+}
+
+int cfdg_solver_profile_read(cfdg_solver* s, double* ms_h, int64_t* launches_h, double* bytes_h) {
+    if (!ms_h || !launches_h) return CFDG_ERR_INVALID;
+    CFDG_SOLVER_CALL(s, {
+        cfdg::cuda_check(cudaStreamSynchronize(s->impl->stream()), "sync");
+        s->impl->profiler().collect();
+        for (int c = 0; c < CFDG_KCAT_COUNT; ++c) {
+            ms_h[c] = s->impl->profiler().ms[c];
+            launches_h[c] = s->impl->profiler().count[c];
+            if (bytes_h) bytes_h[c] = s->impl->profiler().bytes[c];
+        }
+    });
+}
+
+int cfdg_solver_sgs_info(const cfdg_solver* s, int32_t* fwd, int32_t* bwd) {
+    if (!s || !s->impl || !fwd || !bwd) return CFDG_ERR_INVALID;
+    *fwd = s->impl->system().groups_fwd();
+    *bwd = s->impl->system().groups_bwd();
+    return CFDG_OK;
+}
+
+// -------------------------------------------------------------- linalg
+int cfdg_bsr_create(int device, int32_t n_rows, int32_t bs, const int32_t* row_ptr_h, const int32_t* cols_h,
+                    int32_t precision, cfdg_bsr** out) {
+    if (!out || !row_ptr_h || (!cols_h && n_rows > 0)) return CFDG_ERR_INVALID;
+    *out = nullptr;
+    const int dev = require_device(device);
+    if (dev != CFDG_OK) return dev;
+    return guarded([&] {
+        cfdg::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        auto* a = new cfdg_bsr{nullptr, nullptr, device};
+        try {
+            cfdg::cuda_check(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            a->impl = new cfdg::BsrSystem(device, n_rows, bs, row_ptr_h, cols_h, precision, a->stream);
+            cfdg::cuda_check(cudaStreamSynchronize(a->stream), "sync");
+        } catch (...) {
+            if (a->stream) cudaStreamDestroy(a->stream);
+            delete a;
+            throw;
+        }
+        *out = a;
+    });
+}
+
+int cfdg_bsr_destroy(cfdg_bsr* a) {
+    if (!a) return CFDG_OK;
+    const int st = guarded([&] {
+        delete a->impl;
+        if (a->stream) cudaStreamDestroy(a->stream);
+    });
+    delete a;
+    return st;
+}
+
+#define CFDG_BSR_CALL(a, ...)                        \
+    if (!(a) || !(a)->impl) return CFDG_ERR_INVALID; \
+    return guarded([&] { cudaSetDevice((a)->device); __VA_ARGS__; })
+
+int cfdg_bsr_set_values(cfdg_bsr* a, const double* values_h) {
+    if (!values_h) return CFDG_ERR_INVALID;
+    CFDG_BSR_CALL(a, a->impl->set_values_host(values_h); cfdg::cuda_check(cudaStreamSynchronize(a->stream), "sync"));
+}
+
+int cfdg_bsr_spmv(cfdg_bsr* a, const double* x_d, double* y_d, double alpha, double beta) {
+    if (!x_d || !y_d) return CFDG_ERR_INVALID;
+    CFDG_BSR_CALL(a, a->impl->spmv(x_d, y_d, alpha, beta); cfdg::cuda_check(cudaStreamSynchronize(a->stream), "sync"));
+}
+
+namespace {
+struct HostVec {
+    double* d = nullptr;
+    ~HostVec() {
+        if (d) cudaFree(d);
+    }
+    void make(std::size_t n, cudaStream_t s, const double* src) {
+        cfdg::cuda_check(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(double) * (n ? n : 1)), "cudaMalloc");
+        if (src && n) cfdg::cuda_check(cudaMemcpyAsync(d, src, sizeof(double) * n, cudaMemcpyHostToDevice, s), "H2D");
+        else cfdg::cuda_check(cudaMemsetAsync(d, 0, sizeof(double) * (n ? n : 1), s), "memset");
+    }
+    void get(double* dst, std::size_t n, cudaStream_t s) {
+        if (n) cfdg::cuda_check(cudaMemcpyAsync(dst, d, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "D2H");
+        cfdg::cuda_check(cudaStreamSynchronize(s), "sync");
+    }
+};
+}  // namespace
+
+int cfdg_bsr_spmv_host(cfdg_bsr* a, const double* x_h, double* y_h, double alpha, double beta) {
+    if (!x_h || !y_h) return CFDG_ERR_INVALID;
+    CFDG_BSR_CALL(a, {
+        const std::size_t N = static_cast<std::size_t>(a->impl->n()) * a->impl->bs();
+        HostVec x, y;
+        x.make(N, a->stream, x_h);
+        y.make(N, a->stream, y_h);
+        a->impl->spmv(x.d, y.d, alpha, beta);
+        y.get(y_h, N, a->stream);
+    });
+}
+
+int cfdg_sgs_setup(cfdg_bsr* a, int32_t ordering, int32_t sweeps) {
+    CFDG_BSR_CALL(a, a->impl->sgs_setup(ordering, sweeps));
+}
+
+int cfdg_sgs_apply(cfdg_bsr* a, const double* r_d, double* z_d) {
+    if (!r_d || !z_d) return CFDG_ERR_INVALID;
+    CFDG_BSR_CALL(a, a->impl->sgs_apply(r_d, z_d, nullptr); cfdg::cuda_check(cudaStreamSynchronize(a->stream), "sync"));
+}
+
+int cfdg_sgs_apply_host(cfdg_bsr* a, const double* r_h, double* z_h) {
+    if (!r_h || !z_h) return CFDG_ERR_INVALID;
+    CFDG_BSR_CALL(a, {
+        const std::size_t N = static_cast<std::size_t>(a->impl->n()) * a->impl->bs();
+        HostVec r, z;
+        r.make(N, a->stream, r_h);
+        z.make(N, a->stream, nullptr);
+        a->impl->sgs_apply(r.d, z.d, nullptr);
+        z.get(z_h, N, a->stream);
+    });
+}
+
+int cfdg_bicgstab(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it, double* x_d,
+                  const double* b_d, cfdg_krylov_result* out_h) {
+    if (!x_d || !b_d) return CFDG_ERR_INVALID;
+    CFDG_BSR_CALL(a, {
+        const cfdg_krylov_result r = a->impl->bicgstab(precond, rel_tol, abs_tol, max_it, x_d, b_d);
+        if (out_h) *out_h = r;
+    });
+}
+
+int cfdg_bicgstab_host(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it, double* x_h,
+                       const double* b_h, cfdg_krylov_result* out_h) {
+    if (!x_h || !b_h) return CFDG_ERR_INVALID;
+    CFDG_BSR_CALL(a, {
+        const std::size_t N = static_cast<std::size_t>(a->impl->n()) * a->impl->bs();
+        HostVec x, b;
+        x.make(N, a->stream, x_h);
+        b.make(N, a->stream, b_h);
+        const cfdg_krylov_result r = a->impl->bicgstab(precond, rel_tol, abs_tol, max_it, x.d, b.d);
+        x.get(x_h, N, a->stream);
+        if (out_h) *out_h = r;
+    });
+}
+
+}  // extern "C"

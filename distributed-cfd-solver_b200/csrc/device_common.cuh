@@ -1,0 +1,68 @@
+// Device-side data views and launch helpers shared by all kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cfdg {
+
+constexpr int kMaxVars = 6;
+
+// Per-patch boundary data resolved on the host from bc::BCDescriptor the way
+// BoundaryManager::register_all does (include/cfd/solver/compressible/bc_manager.hpp:223-329).
+struct BcPatch {
+    int32_t kind;   // CFDG_BC_* (or -1: patch absent from the configuration)
+    int32_t sa_kind;  // nu_tilde treatment: 0 wall, 1 inflow, 2 outflow, 3 symmetry
+    double qfix[5];   // fixed primitive state (p,u,v,w,T) where the BC has one
+    double p_out;     // subsonic outlet back pressure
+    double tmp_grad;  // heat-flux wall normal temperature gradient
+    double far_p, far_T, far_u, far_v, far_w;  // farfield freestream
+};
+
+// Read-only mesh arrays on the device (single partition, n_own == n_cells).
+struct DevMesh {
+    int32_t n, nf, ni, nb, nt;           // cells, faces, inner faces, boundary faces, n + nb
+    const int32_t* owner;                // nf
+    const int32_t* neigh;                // nf
+    const int32_t* bpatch;               // nb: patch of face ni + b
+    const double *fnx, *fny, *fnz, *farea;      // nf
+    const double *fcx, *fcy, *fcz;              // nf
+    const double *fdx, *fdy, *fdz, *finv_d;     // nf: face-cell distance vectors, 1/|d|
+    const double *ccx, *ccy, *ccz, *vol;        // n
+    const int32_t *c2f_off, *c2f;        // cell -> faces (ascending)
+    const int32_t *c2c_off, *c2c;        // cell -> face neighbours (sorted)
+    const int32_t *g_off, *g_col;        // gradient stencil
+    const double *g_wx, *g_wy, *g_wz;    // LSQ coefficients per stencil entry
+    const BcPatch* patches;
+    int32_t n_patches;
+    const double* wall_dist;             // n (SA)
+};
+
+struct GasParams {
+    double gamma, R, cv, cp, prandtl, prandtl_turb;
+};
+
+// Mutable per-cell/face fields (SoA).  Variable v of q lives at q + v*nt,
+// gradient plane p of variable v at grad + (v*3+p)*nt.
+struct DevFields {
+    double* U;       // nv * n
+    double* q;       // 5 * nt
+    double* grad;    // nv_grad * 3 * nt
+    double* phi;     // 5 * n
+    double* fflux;   // (nv + 1) * nf: face flux per variable, then A*s_max
+    double* res;     // nv * n
+    double* lam;     // n
+    double* dt;      // n
+    double* alpha;   // n
+    // Spalart-Allmaras scratch
+    double* nu;      // nt: specific nu_tilde
+    double* rho;     // nt: density
+    double* mut;     // nt: eddy viscosity
+};
+
+inline unsigned grid_for(int64_t threads, int block) {
+    const int64_t g = (threads + block - 1) / block;
+    return static_cast<unsigned>(g < 1 ? 1 : g);
+}
+
+}  // namespace cfdg

@@ -1,0 +1,87 @@
+// Kernel launchers (host declarations) and device reduction helpers.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+
+namespace cfdg {
+
+#ifdef __CUDACC__
+// Deterministic block reduction of K values: warp shuffle trees, then the
+// warps' results summed in warp order by warp 0.  Thread 0 stores K values.
+template <int K, int BLOCK>
+__device__ __forceinline__ void block_reduce_store(double (&val)[K], double* __restrict__ out) {
+    __shared__ double sh[K][BLOCK / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double x = val[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[k][warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double x = (lane < BLOCK / 32) ? sh[k][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) out[k] = x;
+        }
+    }
+}
+#endif
+
+// ---------------------------------------------------------------- residual
+void launch_primitives(const DevMesh& m, const DevFields& f, const GasParams& g, cudaStream_t s);
+void launch_gradient(const DevMesh& m, const double* src, double* dst, int nvars, cudaStream_t s);
+void launch_limiter_ghostgrad(const DevMesh& m, const DevFields& f, const GasParams& g, bool limit, int limiter,
+                              double venkat_k, cudaStream_t s);
+void launch_face_flux(const DevMesh& m, const DevFields& f, const GasParams& g, bool muscl, bool visc,
+                      cudaStream_t s);
+void launch_cell_residual(const DevMesh& m, const DevFields& f, cudaStream_t s);
+int norm_blocks(int32_t n);
+void launch_norms(int32_t n, int nv, const double* res, double* partials, double* l2, cudaStream_t s);
+void launch_dt_rhs(const DevMesh& m, const DevFields& f, int nv, double cfl, double* b, double* du, cudaStream_t s);
+void launch_state_update(const DevMesh& m, double* U, const double* du, int nv, cudaStream_t s);
+void launch_fill(double* x, int64_t count, double value, cudaStream_t s);
+
+// -------------------------------------------------------- Spalart-Allmaras
+struct SaParams {
+    double nu_inf;      // freestream specific nu_tilde
+    double sigma, cb1, cb2, kappa, cw1, cw2, cw3, cv1;
+};
+void launch_sa_pre(const DevMesh& m, const DevFields& f, const GasParams& g, const SaParams& sa, cudaStream_t s);
+void launch_sa_face_sweep(const DevMesh& m, const DevFields& f, const GasParams& g, const SaParams& sa,
+                          double* sa_face, cudaStream_t s);
+void launch_sa_cell(const DevMesh& m, const DevFields& f, const GasParams& g, const SaParams& sa,
+                    const double* sa_face, cudaStream_t s);
+
+// ---------------------------------------------------------------- Jacobian
+struct JacStructure {
+    const int32_t* row_ptr;   // n+1
+    const int32_t* cols;      // nnzb
+    const int32_t* diag;      // n
+    const int32_t* trans;     // nnzb: position of the transposed block
+    const int32_t* face_pos;  // 2*ni: block (owner,neigh), block (neigh,owner)
+};
+template <typename MT>
+void launch_jacobian(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,
+                     bool visc, MT* values, double* bface_scratch, cudaStream_t s);
+
+// ------------------------------------------------------------ linear algebra
+struct BsrView {
+    int32_t n, bs;
+    const int32_t* row_ptr;
+    const int32_t* cols;
+    const int32_t* diag;
+};
+template <typename MT>
+void launch_lu_setup(const BsrView& A, const MT* vals, MT* lu, int8_t* piv, int* err_flag, cudaStream_t s);
+int spmv_blocks(int32_t n, int32_t bs);
+int dot_blocks(int64_t len);
+
+}  // namespace cfdg

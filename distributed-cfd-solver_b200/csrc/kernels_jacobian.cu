@@ -1,0 +1,174 @@
+// First-order Picard Jacobian assembly into BSR (JacobianKernel::apply,
+// include/cfd/solver/compressible/jacobian_kernel.hpp:74-270).
+//
+// Every off-diagonal block belongs to exactly one interior face, so the face
+// kernel writes it directly at a position precomputed on the host (no
+// binary search, no atomics):  A(c0,c1) = dF/dUR,  A(c1,c0) = -dF/dUL.
+// The diagonal block of cell c is the sum of the owner-side contributions of
+// its faces, which are minus the transposed off-diagonal blocks, plus the
+// boundary-face blocks and alpha*I; the diagonal kernel gathers them in the
+// same order as the sequential reference adds them.
+#include "kernels.hpp"
+#include "physics.cuh"
+
+namespace cfdg {
+
+namespace {
+
+template <typename MT>
+__device__ __forceinline__ MT to_mt(double x) { return static_cast<MT>(x); }
+
+// dF/dU of one side: A*(0.5*J(U) + sgn*0.5*smax*I) (+ viscous, sign vs),
+// HllcFlux::face_flux_jacobian (fluxes/hllc.hpp:135-168),
+// ViscousFlux::face_flux_jacobian (fluxes/viscous.hpp:280-360).
+__device__ __forceinline__ void side_jacobian(const GasParams& g, const double U[5], double nx, double ny, double nz,
+                                              double half_area, double diss, double J[25]) {
+    euler_jacobian(g, U, nx, ny, nz, J);
+#pragma unroll
+    for (int i = 0; i < 25; ++i) J[i] *= half_area;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) J[i * 6] += diss;
+}
+
+template <typename MT, bool VISC, int BS>
+__global__ void __launch_bounds__(128) k_jac_offdiag(DevMesh m, DevFields f, GasParams g, JacStructure js, MT* vals) {
+    const int32_t fc = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fc >= m.ni) return;
+    const int64_t nt = m.nt;
+    const int32_t c0 = m.owner[fc], c1 = m.neigh[fc];
+    const double nx = m.fnx[fc], ny = m.fny[fc], nz = m.fnz[fc], A = m.farea[fc];
+    double qL[5], qR[5], UL[5], UR[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        qL[v] = f.q[v * nt + c0];
+        qR[v] = f.q[v * nt + c1];
+    }
+    prim_to_cons(g, qL[0], qL[1], qL[2], qL[3], qL[4], UL);
+    prim_to_cons(g, qR[0], qR[1], qR[2], qR[3], qR[4], UR);
+    const double smax = hllc_smax(g, UL, UR, nx, ny, nz);
+    const double half_area = 0.5 * A, diss = 0.5 * smax * A;
+    double mutL = 0.0, mutR = 0.0;
+    if (VISC && f.mut) {
+        mutL = f.mut[c0];
+        mutR = f.mut[c1];
+    }
+    double J[25];
+    // A(c0, c1) += dF/dUR
+    side_jacobian(g, UR, nx, ny, nz, half_area, -diss, J);
+    if (VISC) viscous_jacobian_add(g, m.finv_d[fc], qL, qR, mutL, mutR, A, -1.0, J);
+    {
+        MT* dst = vals + int64_t(js.face_pos[2 * fc]) * (BS * BS);
+        if (BS == 5) {
+#pragma unroll
+            for (int i = 0; i < 25; ++i) dst[i] = to_mt<MT>(J[i]);
+        } else {
+#pragma unroll
+            for (int r = 0; r < BS; ++r)
+#pragma unroll
+                for (int c = 0; c < BS; ++c) dst[r * BS + c] = (r < 5 && c < 5) ? to_mt<MT>(J[r * 5 + c]) : MT(0);
+        }
+    }
+    // A(c1, c0) -= dF/dUL
+    side_jacobian(g, UL, nx, ny, nz, half_area, diss, J);
+    if (VISC) viscous_jacobian_add(g, m.finv_d[fc], qL, qR, mutL, mutR, A, 1.0, J);
+    {
+        MT* dst = vals + int64_t(js.face_pos[2 * fc + 1]) * (BS * BS);
+        if (BS == 5) {
+#pragma unroll
+            for (int i = 0; i < 25; ++i) dst[i] = to_mt<MT>(-J[i]);
+        } else {
+#pragma unroll
+            for (int r = 0; r < BS; ++r)
+#pragma unroll
+                for (int c = 0; c < BS; ++c) dst[r * BS + c] = (r < 5 && c < 5) ? to_mt<MT>(-J[r * 5 + c]) : MT(0);
+        }
+    }
+}
+
+// Boundary faces: owner-side block only, first-order states against the BC
+// ghost, ghost eddy viscosity zero (jacobian_kernel.hpp:232-269).
+template <bool VISC>
+__global__ void __launch_bounds__(128) k_jac_bface(DevMesh m, DevFields f, GasParams g, double* __restrict__ out) {
+    const int32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.nb) return;
+    const int64_t nt = m.nt;
+    const int32_t fc = m.ni + b;
+    const int32_t c0 = m.owner[fc];
+    const int64_t cg = int64_t(m.n) + b;
+    const double nx = m.fnx[fc], ny = m.fny[fc], nz = m.fnz[fc], A = m.farea[fc];
+    double qL[5], qR[5], UL[5], UR[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        qL[v] = f.q[v * nt + c0];
+        qR[v] = f.q[v * nt + cg];
+    }
+    prim_to_cons(g, qL[0], qL[1], qL[2], qL[3], qL[4], UL);
+    prim_to_cons(g, qR[0], qR[1], qR[2], qR[3], qR[4], UR);
+    const double smax = hllc_smax(g, UL, UR, nx, ny, nz);
+    double J[25];
+    side_jacobian(g, UL, nx, ny, nz, 0.5 * A, 0.5 * smax * A, J);
+    if (VISC) {
+        const double mutL = f.mut ? f.mut[c0] : 0.0;
+        viscous_jacobian_add(g, m.finv_d[fc], qL, qR, mutL, 0.0, A, 1.0, J);
+    }
+#pragma unroll
+    for (int i = 0; i < 25; ++i) out[int64_t(b) * 25 + i] = J[i];
+}
+
+// Diagonal block entry (c, e): -sum of transposed off-diagonal blocks of row
+// c, + boundary-face blocks, + alpha on the diagonal.  Entries outside the
+// 5x5 mean-flow part (bs = 6) are left to the turbulence assembly.
+template <typename MT, int BS>
+__global__ void __launch_bounds__(256) k_jac_diag(DevMesh m, const double* __restrict__ alpha, JacStructure js,
+                                                  const double* __restrict__ bjac, MT* vals) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= int64_t(m.n) * 25) return;
+    const int32_t c = static_cast<int32_t>(t / 25);
+    const int e = static_cast<int>(t % 25);
+    const int er = e / 5, ec = e % 5;
+    const int eb = er * BS + ec;
+    const int32_t d = js.diag[c];
+    double v = 0.0;
+    for (int32_t k = js.row_ptr[c]; k < js.row_ptr[c + 1]; ++k) {
+        if (k == d) continue;
+        v -= static_cast<double>(vals[int64_t(js.trans[k]) * (BS * BS) + eb]);
+    }
+    for (int32_t q = m.c2f_off[c]; q < m.c2f_off[c + 1]; ++q) {
+        const int32_t fc = m.c2f[q];
+        if (fc >= m.ni) v += bjac[int64_t(fc - m.ni) * 25 + e];
+    }
+    if (er == ec && alpha) v += alpha[c];
+    vals[int64_t(d) * (BS * BS) + eb] = to_mt<MT>(v);
+}
+
+}  // namespace
+
+template <typename MT>
+void launch_jacobian(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,
+                     bool visc, MT* values, double* bface_scratch, cudaStream_t s) {
+    if (m.ni > 0) {
+        const unsigned gr = grid_for(m.ni, 128);
+        if (bs == 5) {
+            if (visc) k_jac_offdiag<MT, true, 5><<<gr, 128, 0, s>>>(m, f, g, js, values);
+            else k_jac_offdiag<MT, false, 5><<<gr, 128, 0, s>>>(m, f, g, js, values);
+        } else {
+            if (visc) k_jac_offdiag<MT, true, 6><<<gr, 128, 0, s>>>(m, f, g, js, values);
+            else k_jac_offdiag<MT, false, 6><<<gr, 128, 0, s>>>(m, f, g, js, values);
+        }
+    }
+    if (m.nb > 0) {
+        const unsigned gr = grid_for(m.nb, 128);
+        if (visc) k_jac_bface<true><<<gr, 128, 0, s>>>(m, f, g, bface_scratch);
+        else k_jac_bface<false><<<gr, 128, 0, s>>>(m, f, g, bface_scratch);
+    }
+    const unsigned gd = grid_for(int64_t(m.n) * 25, 256);
+    if (bs == 5) k_jac_diag<MT, 5><<<gd, 256, 0, s>>>(m, f.alpha, js, bface_scratch, values);
+    else k_jac_diag<MT, 6><<<gd, 256, 0, s>>>(m, f.alpha, js, bface_scratch, values);
+}
+
+template void launch_jacobian<double>(const DevMesh&, const DevFields&, const GasParams&, const JacStructure&, int,
+                                      bool, double*, double*, cudaStream_t);
+template void launch_jacobian<float>(const DevMesh&, const DevFields&, const GasParams&, const JacStructure&, int,
+                                     bool, float*, double*, cudaStream_t);
+
+}  // namespace cfdg

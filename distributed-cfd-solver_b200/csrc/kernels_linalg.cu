@@ -1,0 +1,497 @@
+// Block-sparse linear algebra on the device: BSR SpMV with fused inner
+// products, block LU of the diagonal, SGS sweeps over row lists (levels or
+// colours), and the BiCGSTAB vector kernels with device-side scalar logic.
+//
+// References (maksim-movsisyan/Distributed-cfd-solver):
+//   bsr_spmv<BS>          include/cfd/linalg/bsr_helpers.hpp:138-203
+//   lu_factor_block       include/cfd/linalg/bsr_helpers.hpp:278-321
+//   lu_solve_block<BS>    include/cfd/linalg/bsr_helpers.hpp:324-353
+//   bsr_sgs_sweep<BS>     include/cfd/linalg/bsr_helpers.hpp:389-435
+//   BiCGSTAB::solve       src/linalg/bicgstab.cpp:42-201
+#include "kernels.hpp"
+#include "krylov.hpp"
+
+namespace cfdg {
+
+namespace {
+
+template <typename MT>
+__device__ __forceinline__ double ld(const MT* p) { return static_cast<double>(__ldg(p)); }
+
+// --------------------------------------------------------------- SpMV
+// One thread per (block row, component): y_i[ii] = alpha * sum_k sum_jj
+// A_k[ii][jj] x_col(k)[jj] + beta * y.  Optional fused dot products of y
+// (or other vectors) for the Krylov scalars, reduced per block.
+template <typename MT, int BS, int ND>
+__global__ void __launch_bounds__(256) k_spmv(BsrView A, const MT* __restrict__ vals, const double* __restrict__ x,
+                                              double* __restrict__ y, double alpha, double beta, DotSpec ds,
+                                              double* __restrict__ partials, const int* __restrict__ active) {
+    if (active && *active != 0) return;
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t N = int64_t(A.n) * BS;
+    double yv = 0.0;
+    if (t < N) {
+        const int32_t row = static_cast<int32_t>(t / BS);
+        const int ii = static_cast<int>(t % BS);
+        double acc = 0.0;
+        const int32_t k1 = A.row_ptr[row + 1];
+        for (int32_t k = A.row_ptr[row]; k < k1; ++k) {
+            const MT* a = vals + int64_t(k) * (BS * BS) + ii * BS;
+            const double* xb = x + int64_t(A.cols[k]) * BS;
+            double s = 0.0;
+#pragma unroll
+            for (int jj = 0; jj < BS; ++jj) s += ld(a + jj) * xb[jj];
+            acc += s;
+        }
+        if (alpha == 1.0 && beta == 0.0) yv = acc;
+        else if (beta == 1.0) yv = y[t] + alpha * acc;
+        else if (beta == 0.0) yv = alpha * acc;
+        else yv = alpha * acc + beta * y[t];
+        y[t] = yv;
+    }
+    if constexpr (ND > 0) {
+        double pr[ND];
+#pragma unroll
+        for (int k = 0; k < ND; ++k) {
+            if (t < N) {
+                const double a = ds.a[k] ? ds.a[k][t] : yv;
+                const double b = ds.b[k] ? ds.b[k][t] : yv;
+                pr[k] = a * b;
+            } else {
+                pr[k] = 0.0;
+            }
+        }
+        block_reduce_store<ND, 256>(pr, partials + size_t(blockIdx.x) * ND);
+    }
+}
+
+// -------------------------------------------------------- block LU setup
+template <typename MT, int BS>
+__global__ void k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu, int8_t* __restrict__ piv,
+                     int* __restrict__ err) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    double a[BS * BS];
+    const MT* src = vals + int64_t(A.diag[i]) * (BS * BS);
+#pragma unroll
+    for (int e = 0; e < BS * BS; ++e) a[e] = static_cast<double>(src[e]);
+    int8_t pv[BS];
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < BS; ++k) {
+        int m = k;
+        double mx = fabs(a[k * BS + k]);
+#pragma unroll
+        for (int r = k + 1; r < BS; ++r) {
+            const double v = fabs(a[r * BS + k]);
+            if (v > mx) {
+                mx = v;
+                m = r;
+            }
+        }
+        pv[k] = static_cast<int8_t>(m);
+        if (mx == 0.0) ok = false;
+        if (m != k) {
+#pragma unroll
+            for (int r = k + 1; r < BS; ++r)
+                if (r == m) {
+#pragma unroll
+                    for (int j = 0; j < BS; ++j) {
+                        const double tmp = a[k * BS + j];
+                        a[k * BS + j] = a[r * BS + j];
+                        a[r * BS + j] = tmp;
+                    }
+                }
+        }
+        const double inv_d = 1.0 / a[k * BS + k];
+#pragma unroll
+        for (int r = k + 1; r < BS; ++r) {
+            const double l = a[r * BS + k] * inv_d;
+            a[r * BS + k] = l;
+#pragma unroll
+            for (int j = k + 1; j < BS; ++j) a[r * BS + j] -= l * a[k * BS + j];
+        }
+    }
+    MT* dst = lu + int64_t(i) * (BS * BS);
+#pragma unroll
+    for (int e = 0; e < BS * BS; ++e) dst[e] = static_cast<MT>(a[e]);
+#pragma unroll
+    for (int k = 0; k < BS; ++k) piv[int64_t(i) * BS + k] = pv[k];
+    if (!ok || !isfinite(a[BS * BS - 1])) {
+        atomicCAS(err, 0, i + 1);
+    }
+}
+
+// Pivoted forward/backward substitution of one block (lu_solve_block) in
+// registers; b holds the right-hand side on entry and the solution on exit.
+template <typename MT, int BS>
+__device__ __forceinline__ void lu_solve(const MT* __restrict__ lu, const int8_t* __restrict__ piv, double (&b)[BS]) {
+#pragma unroll
+    for (int k = 0; k < BS; ++k) {
+        const int p = piv[k];
+        double bp = b[k];
+#pragma unroll
+        for (int j = k + 1; j < BS; ++j)
+            if (j == p) bp = b[j];
+        const double bk = b[k];
+        b[k] = bp;
+#pragma unroll
+        for (int j = k + 1; j < BS; ++j)
+            if (j == p) b[j] = bk;
+    }
+#pragma unroll
+    for (int i = 1; i < BS; ++i) {
+        double s = b[i];
+#pragma unroll
+        for (int j = 0; j < i; ++j) s -= ld(lu + i * BS + j) * b[j];
+        b[i] = s;
+    }
+#pragma unroll
+    for (int i = BS - 1; i >= 0; --i) {
+        double s = b[i];
+#pragma unroll
+        for (int j = i + 1; j < BS; ++j) s -= ld(lu + i * BS + j) * b[j];
+        b[i] = s / ld(lu + i * BS + i);
+    }
+}
+
+// One SGS pass over a row list.  A group of BS lanes owns one row: lane ii
+// accumulates component ii of s = r_i - sum_{k != diag} A_ik z_k (columns in
+// ascending order, as the sequential sweep), the group exchanges s by warp
+// shuffles, and each lane solves the pivoted LU system and keeps its entry.
+// MODE 1 skips the neighbour sum (all neighbour z are still zero).
+template <typename MT, int BS, int MODE>
+__global__ void __launch_bounds__(256) k_sgs_rows(BsrView A, const MT* __restrict__ vals, const MT* __restrict__ lu,
+                                                  const int8_t* __restrict__ piv, const int32_t* __restrict__ rows,
+                                                  int32_t n_rows, const double* __restrict__ r, double* __restrict__ z,
+                                                  const int* __restrict__ active) {
+    if (active && *active != 0) return;
+    constexpr int GPW = 32 / BS;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int grp = lane / BS, ii = lane - grp * BS;
+    const int64_t slot = warp * GPW + grp;
+    const bool act = (grp < GPW) && (slot < n_rows);
+    int32_t i = 0;
+    double s = 0.0;
+    if (act) {
+        i = rows[slot];
+        s = r[int64_t(i) * BS + ii];
+        if (MODE == 0) {
+            const int32_t d = A.diag[i];
+            const int32_t k1 = A.row_ptr[i + 1];
+            for (int32_t k = A.row_ptr[i]; k < k1; ++k) {
+                if (k == d) continue;
+                const MT* a = vals + int64_t(k) * (BS * BS) + ii * BS;
+                const double* zb = z + int64_t(A.cols[k]) * BS;
+                double t = 0.0;
+#pragma unroll
+                for (int jj = 0; jj < BS; ++jj) t += ld(a + jj) * zb[jj];
+                s -= t;
+            }
+        }
+    }
+    double b[BS];
+    const int base = (grp < GPW ? grp : 0) * BS;
+#pragma unroll
+    for (int j = 0; j < BS; ++j) b[j] = __shfl_sync(0xffffffffu, s, base + j);
+    if (act) {
+        lu_solve<MT, BS>(lu + int64_t(i) * (BS * BS), piv + int64_t(i) * BS, b);
+        double out = b[0];
+#pragma unroll
+        for (int j = 1; j < BS; ++j)
+            if (j == ii) out = b[j];
+        z[int64_t(i) * BS + ii] = out;
+    }
+}
+
+// ------------------------------------------------------ Krylov kernels
+__global__ void __launch_bounds__(256) k_dot_partials(int64_t len, DotSpec ds, int nd, double* __restrict__ partials) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    double pr[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (t < len) {
+        for (int k = 0; k < nd; ++k) pr[k] = ds.a[k][t] * ds.b[k][t];
+    }
+    block_reduce_store<5, 256>(pr, partials + size_t(blockIdx.x) * 5);
+}
+
+// r = b - v, r0 = r, p = r; partial sums of |b|^2 and |r|^2.
+__global__ void __launch_bounds__(256) k_krylov_init(int64_t len, const double* __restrict__ b, const double* __restrict__ v,
+                                                     double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
+                                                     double* __restrict__ partials) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    double pr[2] = {0.0, 0.0};
+    if (t < len) {
+        const double bt = b[t];
+        const double rt = bt + (-1.0) * v[t];
+        r[t] = rt;
+        r0[t] = rt;
+        p[t] = rt;
+        pr[0] = bt * bt;
+        pr[1] = rt * rt;
+    }
+    block_reduce_store<2, 256>(pr, partials + size_t(blockIdx.x) * 2);
+}
+
+__device__ __forceinline__ double sum_partials(const double* __restrict__ partials, int nblocks, int stride, int k) {
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partials[size_t(b) * stride + k];
+    return s;
+}
+
+__global__ void k_krylov_init_fin(KrylovScalars* ks, const double* __restrict__ partials, int nblocks) {
+    if (threadIdx.x != 0) return;
+    const double bnorm = sqrt(sum_partials(partials, nblocks, 2, 0));
+    const double rnorm = sqrt(sum_partials(partials, nblocks, 2, 1));
+    const double scale = (bnorm > 0.0) ? bnorm : 1.0;
+    ks->bnorm = bnorm;
+    ks->scale = scale;
+    ks->tol = fmax(ks->abs_tol, ks->rel_tol * scale);
+    ks->initial = rnorm;
+    ks->rnorm = rnorm;
+    ks->it = 0;
+    ks->state = KS_RUNNING;
+    if (!isfinite(rnorm)) {
+        ks->state = KS_DIVERGED;
+    } else if (rnorm <= ks->tol) {
+        ks->state = KS_CONVERGED;
+    }
+    ks->rho = rnorm * rnorm;
+    ks->rho_old = 1.0;
+    ks->alpha = 1.0;
+    ks->omega = 1.0;
+    ks->beta = 0.0;
+}
+
+// gamma = r0.v -> alpha = rho / gamma (bicgstab.cpp:112-119); also counts
+// the iteration and stops at max_it.
+__global__ void k_krylov_gamma(KrylovScalars* ks, const double* __restrict__ partials, int nblocks) {
+    if (threadIdx.x != 0 || ks->state != KS_RUNNING) return;
+    const double gamma = sum_partials(partials, nblocks, 1, 0);
+    if (!isfinite(gamma) || gamma == 0.0) {
+        ks->state = KS_DIVERGED;
+        return;
+    }
+    ks->alpha = ks->rho / gamma;
+}
+
+// Iteration gate: stops at max_it before any work of iteration it+1,
+// checks beta of the search direction update (bicgstab.cpp:88-104).
+__global__ void k_krylov_begin(KrylovScalars* ks) {
+    if (threadIdx.x != 0 || ks->state != KS_RUNNING) return;
+    if (ks->it >= ks->max_it) {
+        ks->state = KS_MAXIT;
+        return;
+    }
+    ks->it += 1;
+    if (ks->it > 1 && !isfinite(ks->beta)) ks->state = KS_DIVERGED;
+}
+
+// s = r - alpha v
+__global__ void __launch_bounds__(256) k_krylov_s(int64_t len, const KrylovScalars* __restrict__ ks, const double* __restrict__ r,
+                                                  const double* __restrict__ v, double* __restrict__ s) {
+    if (ks->state != KS_RUNNING) return;
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= len) return;
+    s[t] = r[t] + (-ks->alpha) * v[t];
+}
+
+// Five fused inner products -> omega, reconstructed |r|, rho_next
+// (bicgstab.cpp:128-158), pre-update breakdown checks.
+__global__ void k_krylov_omega(KrylovScalars* ks, const double* __restrict__ partials, int nblocks) {
+    if (threadIdx.x != 0 || ks->state != KS_RUNNING) return;
+    const double tt = sum_partials(partials, nblocks, 5, 0);
+    const double ts = sum_partials(partials, nblocks, 5, 1);
+    const double r0t = sum_partials(partials, nblocks, 5, 2);
+    const double r0s = sum_partials(partials, nblocks, 5, 3);
+    const double ss = sum_partials(partials, nblocks, 5, 4);
+    if (!isfinite(ts) || !isfinite(tt) || tt == 0.0) {
+        ks->state = KS_DIVERGED;
+        return;
+    }
+    const double omega_new = ts / tt;
+    const double rn2 = ss - 2.0 * omega_new * ts + omega_new * omega_new * tt;
+    ks->omega_new = omega_new;
+    ks->rnorm = sqrt(fmax(rn2, 0.0));
+    ks->rho_new = r0s - omega_new * r0t;
+    ks->beta = (ks->rho_new / ks->rho) * (ks->alpha / omega_new);
+}
+
+// x += alpha phat + omega shat; r = s - omega t; next p = r + beta (p - omega v);
+// partial |r|^2 for the periodic true-norm refresh.
+__global__ void __launch_bounds__(256) k_krylov_update(int64_t len, const KrylovScalars* __restrict__ ks,
+                                                       double* __restrict__ x, const double* __restrict__ phat,
+                                                       const double* __restrict__ shat, const double* __restrict__ s,
+                                                       const double* __restrict__ tv, double* __restrict__ r,
+                                                       double* __restrict__ p, const double* __restrict__ v,
+                                                       double* __restrict__ partials) {
+    const bool run = ks->state == KS_RUNNING;
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    double pr[1] = {0.0};
+    if (run && t < len) {
+        const double alpha = ks->alpha, omega = ks->omega_new, beta = ks->beta;
+        double xv = x[t] + alpha * phat[t];
+        xv = xv + omega * shat[t];
+        x[t] = xv;
+        const double rv = s[t] + (-omega) * tv[t];
+        r[t] = rv;
+        double pv = beta * p[t];
+        pv = pv + (-beta * omega) * v[t];
+        pv = pv + 1.0 * rv;
+        p[t] = pv;
+        pr[0] = rv * rv;
+    }
+    if (!run) return;  // uniform across the grid
+    block_reduce_store<1, 256>(pr, partials + size_t(blockIdx.x));
+}
+
+// Post-update checks, refresh every 32 iterations, convergence test
+// (bicgstab.cpp:149-176).
+__global__ void k_krylov_post(KrylovScalars* ks, const double* __restrict__ partials, int nblocks) {
+    if (threadIdx.x != 0 || ks->state != KS_RUNNING) return;
+    const double omega_new = ks->omega_new;
+    double rnorm = ks->rnorm;
+    if (!isfinite(rnorm) || !isfinite(omega_new) || omega_new == 0.0) {
+        ks->state = KS_DIVERGED;
+        return;
+    }
+    if (ks->it % 32 == 0) {
+        rnorm = sqrt(sum_partials(partials, nblocks, 1, 0));
+        ks->rnorm = rnorm;
+    }
+    if (rnorm <= ks->tol) {
+        ks->state = KS_CONVERGED;
+        return;
+    }
+    if (!isfinite(ks->rho_new) || ks->rho_new == 0.0) {
+        ks->state = KS_DIVERGED;
+        return;
+    }
+    ks->rho_old = ks->rho;
+    ks->rho = ks->rho_new;
+    ks->omega = omega_new;
+}
+
+__global__ void k_copy(int64_t len, const double* __restrict__ a, double* __restrict__ b, const int* active) {
+    if (active && *active != 0) return;
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < len) b[t] = a[t];
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers
+int spmv_blocks(int32_t n, int32_t bs) { return static_cast<int>(grid_for(int64_t(n) * bs, 256)); }
+
+template <typename MT>
+void launch_spmv_ex(const BsrView& A, const MT* vals, const double* x, double* y, double alpha, double beta,
+                    const DotSpec& ds, double* partials, const int* active, cudaStream_t s) {
+    const unsigned gr = grid_for(int64_t(A.n) * A.bs, 256);
+    const int nd = ds.n;
+#define CFDG_SPMV(BS, ND) k_spmv<MT, BS, ND><<<gr, 256, 0, s>>>(A, vals, x, y, alpha, beta, ds, partials, active)
+    if (A.bs == 5) {
+        if (nd == 0) CFDG_SPMV(5, 0);
+        else if (nd == 1) CFDG_SPMV(5, 1);
+        else CFDG_SPMV(5, 5);
+    } else if (A.bs == 6) {
+        if (nd == 0) CFDG_SPMV(6, 0);
+        else if (nd == 1) CFDG_SPMV(6, 1);
+        else CFDG_SPMV(6, 5);
+    } else if (A.bs == 1) {
+        if (nd == 0) CFDG_SPMV(1, 0);
+        else if (nd == 1) CFDG_SPMV(1, 1);
+        else CFDG_SPMV(1, 5);
+    } else if (A.bs == 3) {
+        if (nd == 0) CFDG_SPMV(3, 0);
+        else if (nd == 1) CFDG_SPMV(3, 1);
+        else CFDG_SPMV(3, 5);
+    } else if (A.bs == 4) {
+        if (nd == 0) CFDG_SPMV(4, 0);
+        else if (nd == 1) CFDG_SPMV(4, 1);
+        else CFDG_SPMV(4, 5);
+    }
+#undef CFDG_SPMV
+}
+
+template <typename MT>
+void launch_lu_setup(const BsrView& A, const MT* vals, MT* lu, int8_t* piv, int* err_flag, cudaStream_t s) {
+    const unsigned gr = grid_for(A.n, 128);
+    switch (A.bs) {
+        case 1: k_lu<MT, 1><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 3: k_lu<MT, 3><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 4: k_lu<MT, 4><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 5: k_lu<MT, 5><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 6: k_lu<MT, 6><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        default: break;
+    }
+}
+
+template <typename MT>
+void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* rows,
+                        int32_t n_rows, const double* r, double* z, int mode, const int* active, cudaStream_t s) {
+    if (n_rows <= 0) return;
+    const int gpw = 32 / A.bs;
+    const int64_t warps = (int64_t(n_rows) + gpw - 1) / gpw;
+    const unsigned gr = grid_for(warps * 32, 256);
+#define CFDG_SGS(BS)                                                                                          \
+    if (mode == 0) k_sgs_rows<MT, BS, 0><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, n_rows, r, z, active); \
+    else k_sgs_rows<MT, BS, 1><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, n_rows, r, z, active)
+    switch (A.bs) {
+        case 1: CFDG_SGS(1); break;
+        case 3: CFDG_SGS(3); break;
+        case 4: CFDG_SGS(4); break;
+        case 5: CFDG_SGS(5); break;
+        case 6: CFDG_SGS(6); break;
+        default: break;
+    }
+#undef CFDG_SGS
+}
+
+int dot_blocks(int64_t len) { return static_cast<int>(grid_for(len, 256)); }
+
+void launch_dots(int64_t len, const DotSpec& ds, double* partials, cudaStream_t s) {
+    k_dot_partials<<<grid_for(len, 256), 256, 0, s>>>(len, ds, ds.n, partials);
+}
+
+void launch_copy(int64_t len, const double* a, double* b, const int* active, cudaStream_t s) {
+    k_copy<<<grid_for(len, 256), 256, 0, s>>>(len, a, b, active);
+}
+
+void launch_krylov_init(int64_t len, const double* b, const double* v, double* r, double* r0, double* p,
+                        double* partials, KrylovScalars* ks, cudaStream_t s) {
+    const unsigned gr = grid_for(len, 256);
+    k_krylov_init<<<gr, 256, 0, s>>>(len, b, v, r, r0, p, partials);
+    k_krylov_init_fin<<<1, 32, 0, s>>>(ks, partials, static_cast<int>(gr));
+}
+void launch_krylov_begin(KrylovScalars* ks, cudaStream_t s) { k_krylov_begin<<<1, 32, 0, s>>>(ks); }
+void launch_krylov_gamma(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s) {
+    k_krylov_gamma<<<1, 32, 0, s>>>(ks, partials, nblocks);
+}
+void launch_krylov_s(int64_t len, const KrylovScalars* ks, const double* r, const double* v, double* sv,
+                     cudaStream_t s) {
+    k_krylov_s<<<grid_for(len, 256), 256, 0, s>>>(len, ks, r, v, sv);
+}
+void launch_krylov_omega(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s) {
+    k_krylov_omega<<<1, 32, 0, s>>>(ks, partials, nblocks);
+}
+void launch_krylov_update(int64_t len, const KrylovScalars* ks, double* x, const double* phat, const double* shat,
+                          const double* sv, const double* tv, double* r, double* p, const double* v,
+                          double* partials, cudaStream_t s) {
+    k_krylov_update<<<grid_for(len, 256), 256, 0, s>>>(len, ks, x, phat, shat, sv, tv, r, p, v, partials);
+}
+void launch_krylov_post(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s) {
+    k_krylov_post<<<1, 32, 0, s>>>(ks, partials, nblocks);
+}
+
+template void launch_spmv_ex<double>(const BsrView&, const double*, const double*, double*, double, double,
+                                     const DotSpec&, double*, const int*, cudaStream_t);
+template void launch_spmv_ex<float>(const BsrView&, const float*, const double*, double*, double, double,
+                                    const DotSpec&, double*, const int*, cudaStream_t);
+template void launch_lu_setup<double>(const BsrView&, const double*, double*, int8_t*, int*, cudaStream_t);
+template void launch_lu_setup<float>(const BsrView&, const float*, float*, int8_t*, int*, cudaStream_t);
+template void launch_sgs_rows_ex<double>(const BsrView&, const double*, const double*, const int8_t*, const int32_t*,
+                                         int32_t, const double*, double*, int, const int*, cudaStream_t);
+template void launch_sgs_rows_ex<float>(const BsrView&, const float*, const float*, const int8_t*, const int32_t*,
+                                        int32_t, const double*, double*, int, const int*, cudaStream_t);
+
+}  // namespace cfdg

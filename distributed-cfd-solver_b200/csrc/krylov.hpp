@@ -1,0 +1,53 @@
+// Device-resident BiCGSTAB scalars and launcher declarations.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "kernels.hpp"
+
+namespace cfdg {
+
+enum : int { KS_RUNNING = 0, KS_CONVERGED = 1, KS_DIVERGED = 2, KS_MAXIT = 3 };
+
+// Scalars of BiCGSTAB::solve (src/linalg/bicgstab.cpp:42-201) kept on the
+// device so that an iteration needs no host round trip.  `state` is the
+// first member: kernels early-exit when it is not KS_RUNNING.
+struct KrylovScalars {
+    int state;
+    int it;
+    int max_it;
+    int pad_;
+    double rel_tol, abs_tol;
+    double bnorm, scale, tol, initial, rnorm;
+    double rho, rho_old, rho_new, alpha, omega, omega_new, beta;
+};
+
+// Up to five (a, b) vector pairs; a null pointer stands for the SpMV output.
+struct DotSpec {
+    const double* a[5];
+    const double* b[5];
+    int n;
+};
+
+template <typename MT>
+void launch_spmv_ex(const BsrView& A, const MT* vals, const double* x, double* y, double alpha, double beta,
+                    const DotSpec& ds, double* partials, const int* active, cudaStream_t s);
+template <typename MT>
+void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* rows,
+                        int32_t n_rows, const double* r, double* z, int mode, const int* active, cudaStream_t s);
+void launch_dots(int64_t len, const DotSpec& ds, double* partials, cudaStream_t s);
+void launch_copy(int64_t len, const double* a, double* b, const int* active, cudaStream_t s);
+void launch_krylov_init(int64_t len, const double* b, const double* v, double* r, double* r0, double* p,
+                        double* partials, KrylovScalars* ks, cudaStream_t s);
+void launch_krylov_begin(KrylovScalars* ks, cudaStream_t s);
+void launch_krylov_gamma(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s);
+void launch_krylov_s(int64_t len, const KrylovScalars* ks, const double* r, const double* v, double* sv,
+                     cudaStream_t s);
+void launch_krylov_omega(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s);
+void launch_krylov_update(int64_t len, const KrylovScalars* ks, double* x, const double* phat, const double* shat,
+                          const double* sv, const double* tv, double* r, double* p, const double* v,
+                          double* partials, cudaStream_t s);
+void launch_krylov_post(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s);
+
+}  // namespace cfdg

@@ -1,0 +1,1061 @@
+// Host orchestration of the GPU hot path: set-up (connectivity, LSQ
+// coefficients, BSR structure, SGS orderings, boundary table), the residual
+// pipeline, Jacobian assembly, BiCGSTAB + SGS and the Newton loop.
+#include "solver.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace cfdg {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        throw Failure{e == cudaErrorMemoryAllocation ? CFDG_ERR_NOMEM : CFDG_ERR_CUDA,
+                      std::string(what) + ": " + cudaGetErrorString(e)};
+    }
+}
+
+namespace {
+
+template <typename T>
+void upload_or_throw(DevArray<T>& a, const std::vector<T>& h, cudaStream_t s, const char* what) {
+    if (!a.upload(h, s)) throw Failure{CFDG_ERR_NOMEM, std::string("device allocation failed: ") + what};
+}
+template <typename T>
+void alloc_or_throw(DevArray<T>& a, std::size_t n, const char* what) {
+    if (!a.alloc(n)) throw Failure{CFDG_ERR_NOMEM, std::string("device allocation failed: ") + what};
+}
+
+// invert3x3 of the least-squares setup (gradient_operator.cpp:20-47).
+bool invert3x3(const double A[9], double inv[9]) {
+    const double eps = 1.0e-14;
+    const double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+                       A[2] * (A[3] * A[7] - A[4] * A[6]);
+    if (std::abs(det) <= eps) {
+        std::fill_n(inv, 9, 0.0);
+        return false;
+    }
+    const double id = 1.0 / det;
+    inv[0] = (A[4] * A[8] - A[5] * A[7]) * id;
+    inv[1] = (A[2] * A[7] - A[1] * A[8]) * id;
+    inv[2] = (A[1] * A[5] - A[2] * A[4]) * id;
+    inv[3] = (A[5] * A[6] - A[3] * A[8]) * id;
+    inv[4] = (A[0] * A[8] - A[2] * A[6]) * id;
+    inv[5] = (A[2] * A[3] - A[0] * A[5]) * id;
+    inv[6] = (A[3] * A[7] - A[4] * A[6]) * id;
+    inv[7] = (A[1] * A[6] - A[0] * A[7]) * id;
+    inv[8] = (A[0] * A[4] - A[1] * A[3]) * id;
+    return true;
+}
+
+// Weighted least-squares coefficients C_j = A^-1 w_j dr_j, w = 1/|dr|^2,
+// A = sum w dr dr^T + 1e-14 I (LeastSquaresCell{Face,Node}Gradient::setup,
+// gradient_operator.cpp:414-499, 622-707).
+void lsq_coefficients(const HostMesh& m, const Csr& st, std::vector<double>& wx, std::vector<double>& wy,
+                      std::vector<double>& wz) {
+    wx.assign(st.val.size(), 0.0);
+    wy.assign(st.val.size(), 0.0);
+    wz.assign(st.val.size(), 0.0);
+    std::vector<double> dr, w;
+    for (int32_t c = 0; c < m.n_cells; ++c) {
+        const int32_t p1 = st.off[c], p2 = st.off[c + 1];
+        const int32_t nn = p2 - p1;
+        if (nn == 0) continue;
+        const double x0 = m.ccx[c], y0 = m.ccy[c], z0 = m.ccz[c];
+        dr.resize(3 * static_cast<std::size_t>(nn));
+        w.resize(nn);
+        double A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int32_t i = 0; i < nn; ++i) {
+            const int32_t nb = st.val[p1 + i];
+            const double dx = m.ccx[nb] - x0, dy = m.ccy[nb] - y0, dz = m.ccz[nb] - z0;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            const double ww = 1.0 / std::max(r2, 1.0e-30);
+            dr[3 * i] = dx;
+            dr[3 * i + 1] = dy;
+            dr[3 * i + 2] = dz;
+            w[i] = ww;
+            A[0] += ww * dx * dx;
+            A[1] += ww * dx * dy;
+            A[2] += ww * dx * dz;
+            A[4] += ww * dy * dy;
+            A[5] += ww * dy * dz;
+            A[8] += ww * dz * dz;
+        }
+        A[3] = A[1];
+        A[6] = A[2];
+        A[7] = A[5];
+        A[0] += 1.0e-14;
+        A[4] += 1.0e-14;
+        A[8] += 1.0e-14;
+        double inv[9];
+        invert3x3(A, inv);
+        for (int32_t i = 0; i < nn; ++i) {
+            const double rx = w[i] * dr[3 * i], ry = w[i] * dr[3 * i + 1], rz = w[i] * dr[3 * i + 2];
+            wx[p1 + i] = inv[0] * rx + inv[1] * ry + inv[2] * rz;
+            wy[p1 + i] = inv[3] * rx + inv[4] * ry + inv[5] * rz;
+            wz[p1 + i] = inv[6] * rx + inv[7] * ry + inv[8] * rz;
+        }
+    }
+}
+
+struct Inflow {
+    double p, u, v, w, T;
+};
+
+// resolve_inflow of the BC registry (bc_manager.hpp:37-121).
+Inflow resolve_inflow(const cfdg_bc_desc& d, const GasParams& g, double p_ref) {
+    if (d.inflow_mode == CFDG_INFLOW_MACH_ANGLES) {
+        const double k = M_PI / 180.0;
+        const double a_r = d.alpha_deg * k, b_r = d.beta_deg * k;
+        const double rho = p_ref / (g.R * d.t);
+        const double a = std::sqrt(g.gamma * p_ref / rho);
+        const double vm = d.mach * a;
+        return {p_ref, vm * std::cos(a_r) * std::cos(b_r), -vm * std::sin(b_r), vm * std::sin(a_r) * std::cos(b_r),
+                d.t};
+    }
+    if (d.inflow_mode == CFDG_INFLOW_MACH_DIRECTION) {
+        const double rho = p_ref / (g.R * d.t);
+        const double a = std::sqrt(g.gamma * p_ref / rho);
+        const double vm = d.mach * a;
+        const double nrm =
+            std::sqrt(d.direction[0] * d.direction[0] + d.direction[1] * d.direction[1] + d.direction[2] * d.direction[2]);
+        const double inv = (nrm > 1.0e-14) ? (1.0 / nrm) : 0.0;
+        return {p_ref, vm * d.direction[0] * inv, vm * d.direction[1] * inv, vm * d.direction[2] * inv, d.t};
+    }
+    return {p_ref, d.velocity[0], d.velocity[1], d.velocity[2], d.t};
+}
+
+}  // namespace
+
+// =============================================================== Profiler
+Profiler::~Profiler() {
+    for (cudaEvent_t e : all_) cudaEventDestroy(e);
+}
+
+cudaEvent_t Profiler::get() {
+    if (free_.empty()) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        all_.push_back(e);
+        return e;
+    }
+    cudaEvent_t e = free_.back();
+    free_.pop_back();
+    return e;
+}
+
+void Profiler::enable(bool on) {
+    on_ = on;
+    for (int c = 0; c < CFDG_KCAT_COUNT; ++c) {
+        ms[c] = 0.0;
+        count[c] = 0;
+        bytes[c] = 0.0;
+    }
+    for (const Rec& r : pending_) {
+        free_.push_back(r.a);
+        free_.push_back(r.b);
+    }
+    pending_.clear();
+}
+
+void Profiler::start(int cat, cudaStream_t s) {
+    open_ = get();
+    open_cat_ = cat;
+    cuda_check(cudaEventRecord(open_, s), "cudaEventRecord");
+}
+
+void Profiler::stop(cudaStream_t s) {
+    cudaEvent_t b = get();
+    cuda_check(cudaEventRecord(b, s), "cudaEventRecord");
+    pending_.push_back({open_cat_, open_, b});
+    open_ = nullptr;
+}
+
+void Profiler::collect() {
+    for (const Rec& r : pending_) {
+        float t = 0.0f;
+        cuda_check(cudaEventSynchronize(r.b), "cudaEventSynchronize");
+        cuda_check(cudaEventElapsedTime(&t, r.a, r.b), "cudaEventElapsedTime");
+        ms[r.cat] += t;
+        count[r.cat] += 1;
+        free_.push_back(r.a);
+        free_.push_back(r.b);
+    }
+    pending_.clear();
+}
+
+// =============================================================== BsrSystem
+BsrSystem::BsrSystem(int device, int32_t n, int32_t bs, const int32_t* row_ptr, const int32_t* cols, int precision,
+                     cudaStream_t stream)
+    : device_(device), stream_(stream), n_(n), bs_(bs), precision_(precision) {
+    if (n < 0 || bs < 1 || bs > 6 || bs == 2) throw Failure{CFDG_ERR_INVALID, "unsupported BSR size or block size"};
+    row_ptr_h_.assign(row_ptr, row_ptr + n + 1);
+    nnzb_ = row_ptr_h_[n];
+    cols_h_.assign(cols, cols + nnzb_);
+    diag_h_.assign(n, -1);
+    for (int32_t i = 0; i < n; ++i) {
+        if (row_ptr_h_[i + 1] < row_ptr_h_[i]) throw Failure{CFDG_ERR_INVALID, "row pointers must not decrease"};
+        for (int32_t k = row_ptr_h_[i]; k < row_ptr_h_[i + 1]; ++k) {
+            if (cols_h_[k] < 0 || cols_h_[k] >= n) throw Failure{CFDG_ERR_INVALID, "column index out of range"};
+            if (k > row_ptr_h_[i] && cols_h_[k] <= cols_h_[k - 1])
+                throw Failure{CFDG_ERR_INVALID, "columns must be sorted and unique within a row"};
+            if (cols_h_[k] == i) diag_h_[i] = k;
+        }
+        if (diag_h_[i] < 0) throw Failure{CFDG_ERR_INVALID, "block row without a diagonal block"};
+    }
+    upload_or_throw(row_ptr_, row_ptr_h_, stream_, "row_ptr");
+    upload_or_throw(cols_, cols_h_, stream_, "cols");
+    upload_or_throw(diag_, diag_h_, stream_, "diag");
+    const std::size_t nv = static_cast<std::size_t>(nnzb_) * bs * bs;
+    if (precision_ == CFDG_PREC_MIXED) alloc_or_throw(vals32_, nv, "values");
+    else alloc_or_throw(vals64_, nv, "values");
+    const std::size_t N = static_cast<std::size_t>(n) * bs;
+    for (DevArray<double>* a : {&r_, &r0_, &p_, &v_, &s_, &t_, &phat_, &shat_}) alloc_or_throw(*a, N > 0 ? N : 1, "krylov");
+    alloc_or_throw(partials_, static_cast<std::size_t>(std::max(dot_blocks(N), spmv_blocks(n, bs))) * 5 + 8, "partials");
+    alloc_or_throw(ks_, 1, "krylov scalars");
+    alloc_or_throw(err_, 1, "error flag");
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&ks_host_), sizeof(KrylovScalars)), "cudaMallocHost");
+}
+
+BsrSystem::~BsrSystem() {
+    if (ks_host_) cudaFreeHost(ks_host_);
+}
+
+void BsrSystem::set_values_host(const double* v) {
+    const std::size_t nv = static_cast<std::size_t>(nnzb_) * bs_ * bs_;
+    if (precision_ == CFDG_PREC_MIXED) {
+        std::vector<float> f(v, v + nv);
+        cuda_check(cudaMemcpyAsync(vals32_.p, f.data(), nv * sizeof(float), cudaMemcpyHostToDevice, stream_), "H2D");
+        cuda_check(cudaStreamSynchronize(stream_), "sync");
+    } else {
+        cuda_check(cudaMemcpyAsync(vals64_.p, v, nv * sizeof(double), cudaMemcpyHostToDevice, stream_), "H2D");
+    }
+    lu_ready_ = false;
+}
+
+void BsrSystem::get_values_host(double* v) {
+    const std::size_t nv = static_cast<std::size_t>(nnzb_) * bs_ * bs_;
+    if (precision_ == CFDG_PREC_MIXED) {
+        std::vector<float> f(nv);
+        cuda_check(cudaMemcpyAsync(f.data(), vals32_.p, nv * sizeof(float), cudaMemcpyDeviceToHost, stream_), "D2H");
+        cuda_check(cudaStreamSynchronize(stream_), "sync");
+        for (std::size_t i = 0; i < nv; ++i) v[i] = f[i];
+    } else {
+        cuda_check(cudaMemcpyAsync(v, vals64_.p, nv * sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H");
+        cuda_check(cudaStreamSynchronize(stream_), "sync");
+    }
+}
+
+// nnzb blocks + columns, row pointers, x and y once, plus the distinct
+// vectors read by the fused inner products.
+double BsrSystem::spmv_bytes(int n_extra_vectors, bool read_y) const {
+    const double sa = (precision_ == CFDG_PREC_MIXED) ? 4.0 : 8.0;
+    const double N = double(n_) * bs_;
+    return double(nnzb_) * (double(bs_) * bs_ * sa + 4.0) + (n_ + 1.0) * 4.0 + N * 8.0 * (2.0 + (read_y ? 1.0 : 0.0)) +
+           N * 8.0 * n_extra_vectors;
+}
+
+void BsrSystem::spmv(const double* x, double* y, double alpha, double beta) {
+    DotSpec ds{};
+    ds.n = 0;
+    ProfScope ps(prof_, CFDG_KCAT_SPMV, stream_, 1, spmv_bytes(0, beta != 0.0));
+    if (precision_ == CFDG_PREC_MIXED) launch_spmv_ex<float>(view(), vals32_.p, x, y, alpha, beta, ds, nullptr, nullptr, stream_);
+    else launch_spmv_ex<double>(view(), vals64_.p, x, y, alpha, beta, ds, nullptr, nullptr, stream_);
+    cuda_check(cudaGetLastError(), "spmv launch");
+}
+
+// Row groups of the sweep.  LEVEL: level sets of the lower (forward) and
+// upper (backward) dependency graphs, so a level-by-level sweep performs
+// exactly the arithmetic of the sequential sweep.  COLOR: greedy colouring
+// in row order; forward visits colours ascending, backward descending.
+void BsrSystem::build_ordering(int ordering) {
+    const int32_t n = n_;
+    std::vector<int32_t> fwd_key(n, 0), bwd_key(n, 0);
+    if (ordering == CFDG_SGS_LEVEL) {
+        for (int32_t i = 0; i < n; ++i) {
+            int32_t l = 0;
+            for (int32_t k = row_ptr_h_[i]; k < row_ptr_h_[i + 1]; ++k) {
+                const int32_t j = cols_h_[k];
+                if (j < i) l = std::max(l, fwd_key[j] + 1);
+            }
+            fwd_key[i] = l;
+        }
+        for (int32_t i = n - 1; i >= 0; --i) {
+            int32_t l = 0;
+            for (int32_t k = row_ptr_h_[i]; k < row_ptr_h_[i + 1]; ++k) {
+                const int32_t j = cols_h_[k];
+                if (j > i) l = std::max(l, bwd_key[j] + 1);
+            }
+            bwd_key[i] = l;
+        }
+    } else {
+        std::vector<int32_t> color(n, -1);
+        std::vector<char> used;
+        int32_t ncol = 0;
+        for (int32_t i = 0; i < n; ++i) {
+            used.assign(static_cast<std::size_t>(ncol) + 1, 0);
+            for (int32_t k = row_ptr_h_[i]; k < row_ptr_h_[i + 1]; ++k) {
+                const int32_t j = cols_h_[k];
+                if (j != i && color[j] >= 0) used[color[j]] = 1;
+            }
+            int32_t c = 0;
+            while (used[c]) ++c;
+            color[i] = c;
+            ncol = std::max(ncol, c + 1);
+        }
+        for (int32_t i = 0; i < n; ++i) {
+            fwd_key[i] = color[i];
+            bwd_key[i] = ncol - 1 - color[i];
+        }
+    }
+    auto group = [&](const std::vector<int32_t>& key, std::vector<int32_t>& off, std::vector<int32_t>& rows) {
+        int32_t ng = 0;
+        for (int32_t i = 0; i < n; ++i) ng = std::max(ng, key[i] + 1);
+        off.assign(static_cast<std::size_t>(ng) + 1, 0);
+        for (int32_t i = 0; i < n; ++i) ++off[key[i] + 1];
+        for (int32_t g = 0; g < ng; ++g) off[g + 1] += off[g];
+        rows.resize(n);
+        std::vector<int32_t> cur(off.begin(), off.end() - 1);
+        for (int32_t i = 0; i < n; ++i) rows[cur[key[i]]++] = i;
+    };
+    std::vector<int32_t> fr, br;
+    group(fwd_key, fwd_off_, fr);
+    group(bwd_key, bwd_off_, br);
+    // Unique-touch bytes of one pass over a group: row list, row pointers,
+    // diagonal index, off-diagonal blocks + columns, LU + pivots, r, z write,
+    // and each distinct neighbour z block once.
+    const double sa = (precision_ == CFDG_PREC_MIXED) ? 4.0 : 8.0;
+    const double b2 = double(bs_) * bs_;
+    auto pass_bytes = [&](const std::vector<int32_t>& off, const std::vector<int32_t>& rows, std::vector<double>* out) {
+        const int ng = static_cast<int>(off.size()) - 1;
+        out[0].assign(ng, 0.0);
+        out[1].assign(ng, 0.0);
+        std::vector<int32_t> seen(n, -1);
+        for (int g = 0; g < ng; ++g) {
+            double offd = 0.0, nbr = 0.0;
+            const double R = off[g + 1] - off[g];
+            for (int32_t q = off[g]; q < off[g + 1]; ++q) {
+                const int32_t i = rows[q];
+                offd += row_ptr_h_[i + 1] - row_ptr_h_[i] - 1;
+                for (int32_t k = row_ptr_h_[i]; k < row_ptr_h_[i + 1]; ++k) {
+                    const int32_t j = cols_h_[k];
+                    if (j != i && seen[j] != g) {
+                        seen[j] = g;
+                        nbr += 1.0;
+                    }
+                }
+            }
+            const double own = R * (4.0 + b2 * sa + bs_ + 2.0 * 8.0 * bs_);  // list, LU, piv, r, z
+            out[1][g] = own;
+            out[0][g] = own + R * (8.0 + 4.0) + offd * (b2 * sa + 4.0) + nbr * 8.0 * bs_;
+        }
+    };
+    pass_bytes(fwd_off_, fr, fwd_bytes_);
+    pass_bytes(bwd_off_, br, bwd_bytes_);
+    upload_or_throw(fwd_rows_, fr, stream_, "sgs rows");
+    upload_or_throw(bwd_rows_, br, stream_, "sgs rows");
+    ordering_ = ordering;
+}
+
+void BsrSystem::sgs_setup(int ordering, int sweeps) {
+    if (ordering != CFDG_SGS_LEVEL && ordering != CFDG_SGS_COLOR) throw Failure{CFDG_ERR_INVALID, "unknown SGS ordering"};
+    if (sweeps < 1) throw Failure{CFDG_ERR_INVALID, "SGS sweeps must be >= 1"};
+    if (ordering != ordering_) build_ordering(ordering);
+    sweeps_ = sweeps;
+    const std::size_t nb2 = static_cast<std::size_t>(n_) * bs_ * bs_;
+    if (!piv_.p && n_ > 0) alloc_or_throw(piv_, static_cast<std::size_t>(n_) * bs_, "pivots");
+    cuda_check(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_), "memset");
+    if (precision_ == CFDG_PREC_MIXED) {
+        if (!lu32_.p && n_ > 0) alloc_or_throw(lu32_, nb2, "lu");
+        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1, double(n_) * (bs_ * bs_ * 8.0 + bs_ + 4.0));
+        launch_lu_setup<float>(view(), vals32_.p, lu32_.p, piv_.p, err_.p, stream_);
+    } else {
+        if (!lu64_.p && n_ > 0) alloc_or_throw(lu64_, nb2, "lu");
+        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1, double(n_) * (bs_ * bs_ * 16.0 + bs_ + 4.0));
+        launch_lu_setup<double>(view(), vals64_.p, lu64_.p, piv_.p, err_.p, stream_);
+    }
+    cuda_check(cudaGetLastError(), "lu launch");
+    int err = 0;
+    cuda_check(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    cuda_check(cudaStreamSynchronize(stream_), "lu sync");
+    if (err != 0) {
+        throw Failure{CFDG_ERR_SINGULAR, "SgsPreconditioner: singular diagonal block at row " + std::to_string(err - 1)};
+    }
+    lu_ready_ = true;
+}
+
+template <typename MT>
+void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, double* z, const int* active) {
+    const BsrView A = view();
+    const int nf = groups_fwd(), nbk = groups_bwd();
+    const bool color = ordering_ == CFDG_SGS_COLOR;
+    // Neighbours ahead of the cursor must read zero on the first forward
+    // sweep; with two colours every neighbour of the second colour is of the
+    // first colour, so no clearing is needed.
+    if (!color || nf > 2) {
+        ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 0, 8.0 * n_ * bs_);
+        cuda_check(cudaMemsetAsync(z, 0, sizeof(double) * static_cast<std::size_t>(n_) * bs_, stream_), "memset");
+    }
+    for (int sw = 0; sw < sweeps_; ++sw) {
+        for (int g = 0; g < nf; ++g) {
+            int mode = 0;
+            if (color) {
+                if (sw > 0 && g == 0) continue;  // equal to the last backward colour pass
+                if (sw == 0 && g == 0) mode = 1; // all neighbours still zero
+            }
+            ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, fwd_bytes_[mode][g]);
+            launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, fwd_rows_.p + fwd_off_[g], fwd_off_[g + 1] - fwd_off_[g], r,
+                                   z, mode, active, stream_);
+        }
+        for (int g = 0; g < nbk; ++g) {
+            if (color && g == 0) continue;  // first backward colour == last forward colour
+            ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, bwd_bytes_[0][g]);
+            launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, bwd_rows_.p + bwd_off_[g], bwd_off_[g + 1] - bwd_off_[g], r,
+                                   z, 0, active, stream_);
+        }
+    }
+}
+
+void BsrSystem::sgs_apply(const double* r, double* z, const int* active) {
+    if (!lu_ready_) throw Failure{CFDG_ERR_INVALID, "SgsPreconditioner: setup() was not called"};
+    if (precision_ == CFDG_PREC_MIXED) sgs_apply_t<float>(vals32_.p, lu32_.p, r, z, active);
+    else sgs_apply_t<double>(vals64_.p, lu64_.p, r, z, active);
+    cuda_check(cudaGetLastError(), "sgs launch");
+}
+
+cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_tol, int max_it, double* x,
+                                       const double* b) {
+    if (precond == CFDG_PC_SGS && !lu_ready_) throw Failure{CFDG_ERR_INVALID, "SGS preconditioner not set up"};
+    const int64_t N = int64_t(n_) * bs_;
+    const BsrView A = view();
+    const bool mixed = precision_ == CFDG_PREC_MIXED;
+    KrylovScalars init{};
+    init.max_it = max_it;
+    init.rel_tol = rel_tol;
+    init.abs_tol = abs_tol;
+    cuda_check(cudaMemcpyAsync(ks_.p, &init, sizeof(init), cudaMemcpyHostToDevice, stream_), "H2D");
+    const int* active = &ks_.p->state;
+    auto spmv_dots = [&](const double* xin, double* yout, const DotSpec& ds) {
+        ProfScope ps(prof_, CFDG_KCAT_SPMV, stream_, 1, spmv_bytes(ds.n == 1 ? 1 : 2, false));
+        if (mixed) launch_spmv_ex<float>(A, vals32_.p, xin, yout, 1.0, 0.0, ds, partials_.p, active, stream_);
+        else launch_spmv_ex<double>(A, vals64_.p, xin, yout, 1.0, 0.0, ds, partials_.p, active, stream_);
+    };
+    // r = b - A x; r0 = r; p = r
+    {
+        DotSpec none{};
+        none.n = 0;
+        {
+            ProfScope ps(prof_, CFDG_KCAT_SPMV, stream_, 1, spmv_bytes(0, false));
+            if (mixed) launch_spmv_ex<float>(A, vals32_.p, x, v_.p, 1.0, 0.0, none, nullptr, nullptr, stream_);
+            else launch_spmv_ex<double>(A, vals64_.p, x, v_.p, 1.0, 0.0, none, nullptr, nullptr, stream_);
+        }
+        ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 2, 5.0 * 8.0 * N);
+        launch_krylov_init(N, b, v_.p, r_.p, r0_.p, p_.p, partials_.p, ks_.p, stream_);
+    }
+    const int nblk = spmv_blocks(n_, bs_);
+    const int nvec = dot_blocks(N);
+    int it = 0;
+    bool done = false;
+    while (!done && it < max_it) {
+        {
+            ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_);
+            launch_krylov_begin(ks_.p, stream_);
+        }
+        double* phat = p_.p;
+        if (precond == CFDG_PC_SGS) {
+            sgs_apply(p_.p, phat_.p, active);
+            phat = phat_.p;
+        }
+        DotSpec d1{};
+        d1.n = 1;
+        d1.a[0] = r0_.p;
+        d1.b[0] = nullptr;
+        spmv_dots(phat, v_.p, d1);
+        {
+            ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 2, 3.0 * 8.0 * N);
+            launch_krylov_gamma(ks_.p, partials_.p, nblk, stream_);
+            launch_krylov_s(N, ks_.p, r_.p, v_.p, s_.p, stream_);
+        }
+        double* shat = s_.p;
+        if (precond == CFDG_PC_SGS) {
+            sgs_apply(s_.p, shat_.p, active);
+            shat = shat_.p;
+        }
+        DotSpec d5{};
+        d5.n = 5;
+        d5.a[0] = nullptr; d5.b[0] = nullptr;   // t.t
+        d5.a[1] = nullptr; d5.b[1] = s_.p;      // t.s
+        d5.a[2] = r0_.p;   d5.b[2] = nullptr;   // r0.t
+        d5.a[3] = r0_.p;   d5.b[3] = s_.p;      // r0.s
+        d5.a[4] = s_.p;    d5.b[4] = s_.p;      // s.s
+        spmv_dots(shat, t_.p, d5);
+        {
+            ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 3, 10.0 * 8.0 * N);
+            launch_krylov_omega(ks_.p, partials_.p, nblk, stream_);
+            launch_krylov_update(N, ks_.p, x, phat, shat, s_.p, t_.p, r_.p, p_.p, v_.p, partials_.p, stream_);
+            launch_krylov_post(ks_.p, partials_.p, nvec, stream_);
+        }
+        ++it;
+        if (it % check_every == 0 || it == max_it) {
+            cuda_check(cudaMemcpyAsync(ks_host_, ks_.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, stream_), "D2H");
+            cuda_check(cudaStreamSynchronize(stream_), "krylov sync");
+            if (ks_host_->state != KS_RUNNING) done = true;
+        }
+    }
+    {
+        ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_);
+        launch_krylov_begin(ks_.p, stream_);  // marks max-iterations when still running
+    }
+    cuda_check(cudaGetLastError(), "krylov launch");
+    cuda_check(cudaMemcpyAsync(ks_host_, ks_.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, stream_), "D2H");
+    cuda_check(cudaStreamSynchronize(stream_), "krylov sync");
+    cfdg_krylov_result res{};
+    switch (ks_host_->state) {
+        case KS_CONVERGED: res.status = CFDG_KRYLOV_CONVERGED; break;
+        case KS_DIVERGED: res.status = CFDG_KRYLOV_DIVERGED; break;
+        default: res.status = CFDG_KRYLOV_MAX_ITERATIONS; break;
+    }
+    if (max_it <= 0 && ks_host_->state == KS_RUNNING) res.status = CFDG_KRYLOV_MAX_ITERATIONS;
+    res.iterations = ks_host_->it;
+    res.initial_residual = ks_host_->initial;
+    res.final_residual = ks_host_->rnorm;
+    return res;
+}
+
+// ================================================================= Solver
+Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, const cfdg_bc_desc* bcs, int n_bcs)
+    : device_(device), cfg_(cfg) {
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    gas_.gamma = cfg.gamma;
+    gas_.R = cfg.gas_constant;
+    gas_.cv = cfg.gas_constant / (cfg.gamma - 1.0);
+    gas_.cp = cfg.gamma * gas_.cv;
+    gas_.prandtl = cfg.prandtl;
+    gas_.prandtl_turb = cfg.prandtl_turb;
+    sa_ = cfg.turbulence == 1;
+    if (sa_ && !cfg.viscous) throw Failure{CFDG_ERR_INVALID, "Spalart-Allmaras needs the viscous equations"};
+    nv_ = sa_ ? 6 : 5;
+    muscl_ = cfg.reconstruction == CFDG_RECON_MUSCL;
+    need_grad_ = muscl_ || cfg.viscous;
+    if (cfg.gradient != CFDG_GRAD_LSQ_FACE && cfg.gradient != CFDG_GRAD_LSQ_NODE && need_grad_)
+        throw Failure{CFDG_ERR_UNSUPPORTED, "gradient operator not built (least-squares face or node only)"};
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&l2_host_), sizeof(double) * 8), "cudaMallocHost");
+
+    HostMesh hm;
+    hm.from_view(mesh);
+    if (hm.n_cells <= 0 || hm.n_faces <= 0 || hm.n_inner < 0 || hm.n_inner > hm.n_faces)
+        throw Failure{CFDG_ERR_MESH, "empty or inconsistent mesh"};
+    for (int32_t f = 0; f < hm.n_faces; ++f) {
+        const bool inner = f < hm.n_inner;
+        if (hm.owner[f] < 0 || hm.owner[f] >= hm.n_cells) throw Failure{CFDG_ERR_MESH, "face owner out of range"};
+        if (inner && (hm.neigh[f] < 0 || hm.neigh[f] >= hm.n_cells)) throw Failure{CFDG_ERR_MESH, "interior face without neighbour"};
+        if (!inner && hm.neigh[f] >= 0) throw Failure{CFDG_ERR_MESH, "boundary face with a neighbour (3-zone order broken)"};
+        if (!inner && (hm.patch[f] < 0)) throw Failure{CFDG_ERR_MESH, "boundary face without patch"};
+        if (!(hm.area[f] > 1e-15)) throw Failure{CFDG_ERR_MESH, "zero-area face"};
+    }
+    for (int32_t c = 0; c < hm.n_cells; ++c)
+        if (!(hm.vol[c] > 1e-15)) throw Failure{CFDG_ERR_MESH, "non-positive cell volume"};
+    for (int32_t f = hm.n_inner + 1; f < hm.n_faces; ++f)
+        if (hm.patch[f] < hm.patch[f - 1]) throw Failure{CFDG_ERR_MESH, "boundary faces not grouped by patch"};
+
+    setup_mesh(mesh);
+    setup_bcs(bcs, n_bcs, hm);
+    const Csr c2c = build_cell_cells_face(hm);
+    setup_matrix(hm, c2c);
+    sys_->set_profiler(&prof_);
+    {
+        const Csr c2f = build_cell_faces(hm);
+        const int64_t E = need_grad_ ? static_cast<int64_t>(g_col_.count) : 0;
+        compute_alg_bytes(E, static_cast<int64_t>(c2c.val.size()), static_cast<int64_t>(c2f.val.size()));
+    }
+    if (sa_) setup_sa(hm);
+    cuda_check(cudaStreamSynchronize(stream_), "setup sync");
+}
+
+Solver::~Solver() {
+    if (l2_host_) cudaFreeHost(l2_host_);
+    sys_.reset();
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Solver::setup_mesh(const cfdg_mesh_host& mesh) {
+    HostMesh hm;
+    hm.from_view(mesh);
+    const int32_t n = hm.n_cells, nf = hm.n_faces, ni = hm.n_inner, nb = nf - ni;
+    dm_.n = n;
+    dm_.nf = nf;
+    dm_.ni = ni;
+    dm_.nb = nb;
+    dm_.nt = n + nb;
+    cudaStream_t s = stream_;
+    upload_or_throw(owner_, hm.owner, s, "owner");
+    upload_or_throw(neigh_, hm.neigh, s, "neigh");
+    std::vector<int32_t> bp(hm.patch.begin() + ni, hm.patch.end());
+    upload_or_throw(bpatch_, bp, s, "bpatch");
+    upload_or_throw(fnx_, hm.fnx, s, "fnx");
+    upload_or_throw(fny_, hm.fny, s, "fny");
+    upload_or_throw(fnz_, hm.fnz, s, "fnz");
+    upload_or_throw(farea_, hm.area, s, "area");
+    upload_or_throw(fcx_, hm.fcx, s, "fcx");
+    upload_or_throw(fcy_, hm.fcy, s, "fcy");
+    upload_or_throw(fcz_, hm.fcz, s, "fcz");
+    upload_or_throw(ccx_, hm.ccx, s, "ccx");
+    upload_or_throw(ccy_, hm.ccy, s, "ccy");
+    upload_or_throw(ccz_, hm.ccz, s, "ccz");
+    upload_or_throw(vol_, hm.vol, s, "vol");
+    // face-cell distance vectors (build_face_cell_dist_vectors,
+    // src/mesh/aux_geometry.cpp:11-51) and 1/|d| (build_face_cell_dist_inv :107-156)
+    std::vector<double> dx(nf), dy(nf), dz(nf), dinv(nf);
+    for (int32_t f = 0; f < nf; ++f) {
+        const int32_t u = hm.owner[f];
+        if (f < ni) {
+            const int32_t v = hm.neigh[f];
+            dx[f] = hm.ccx[v] - hm.ccx[u];
+            dy[f] = hm.ccy[v] - hm.ccy[u];
+            dz[f] = hm.ccz[v] - hm.ccz[u];
+            const double d = std::sqrt((hm.ccx[v] - hm.ccx[u]) * (hm.ccx[v] - hm.ccx[u]) +
+                                       (hm.ccy[v] - hm.ccy[u]) * (hm.ccy[v] - hm.ccy[u]) +
+                                       (hm.ccz[v] - hm.ccz[u]) * (hm.ccz[v] - hm.ccz[u]));
+            dinv[f] = 1.0 / d;
+        } else {
+            dx[f] = 2.0 * (hm.fcx[f] - hm.ccx[u]);
+            dy[f] = 2.0 * (hm.fcy[f] - hm.ccy[u]);
+            dz[f] = 2.0 * (hm.fcz[f] - hm.ccz[u]);
+            const double d = std::sqrt(4.0 * (hm.fcx[f] - hm.ccx[u]) * (hm.fcx[f] - hm.ccx[u]) +
+                                       4.0 * (hm.fcy[f] - hm.ccy[u]) * (hm.fcy[f] - hm.ccy[u]) +
+                                       4.0 * (hm.fcz[f] - hm.ccz[u]) * (hm.fcz[f] - hm.ccz[u]));
+            dinv[f] = 1.0 / d;
+        }
+    }
+    upload_or_throw(fdx_, dx, s, "fdx");
+    upload_or_throw(fdy_, dy, s, "fdy");
+    upload_or_throw(fdz_, dz, s, "fdz");
+    upload_or_throw(finv_d_, dinv, s, "finv_d");
+    const Csr c2f = build_cell_faces(hm);
+    upload_or_throw(c2f_off_, c2f.off, s, "c2f_off");
+    upload_or_throw(c2f_, c2f.val, s, "c2f");
+    const Csr c2c = build_cell_cells_face(hm);
+    upload_or_throw(c2c_off_, c2c.off, s, "c2c_off");
+    upload_or_throw(c2c_, c2c.val, s, "c2c");
+    if (need_grad_) {
+        const Csr st = (cfg_.gradient == CFDG_GRAD_LSQ_FACE) ? c2c : build_cell_cells_node(hm);
+        std::vector<double> wx, wy, wz;
+        lsq_coefficients(hm, st, wx, wy, wz);
+        upload_or_throw(g_off_, st.off, s, "g_off");
+        upload_or_throw(g_col_, st.val, s, "g_col");
+        upload_or_throw(g_wx_, wx, s, "g_wx");
+        upload_or_throw(g_wy_, wy, s, "g_wy");
+        upload_or_throw(g_wz_, wz, s, "g_wz");
+        // the host vectors die at scope end: make the copies complete first
+        cuda_check(cudaStreamSynchronize(s), "setup sync");
+    }
+    cuda_check(cudaStreamSynchronize(s), "setup sync");
+    dm_.owner = owner_.p;
+    dm_.neigh = neigh_.p;
+    dm_.bpatch = bpatch_.p;
+    dm_.fnx = fnx_.p;
+    dm_.fny = fny_.p;
+    dm_.fnz = fnz_.p;
+    dm_.farea = farea_.p;
+    dm_.fcx = fcx_.p;
+    dm_.fcy = fcy_.p;
+    dm_.fcz = fcz_.p;
+    dm_.fdx = fdx_.p;
+    dm_.fdy = fdy_.p;
+    dm_.fdz = fdz_.p;
+    dm_.finv_d = finv_d_.p;
+    dm_.ccx = ccx_.p;
+    dm_.ccy = ccy_.p;
+    dm_.ccz = ccz_.p;
+    dm_.vol = vol_.p;
+    dm_.c2f_off = c2f_off_.p;
+    dm_.c2f = c2f_.p;
+    dm_.c2c_off = c2c_off_.p;
+    dm_.c2c = c2c_.p;
+    dm_.g_off = g_off_.p;
+    dm_.g_col = g_col_.p;
+    dm_.g_wx = g_wx_.p;
+    dm_.g_wy = g_wy_.p;
+    dm_.g_wz = g_wz_.p;
+
+    // fields
+    const std::size_t nt = static_cast<std::size_t>(dm_.nt), nn = static_cast<std::size_t>(n);
+    alloc_or_throw(U_, nn * nv_, "U");
+    alloc_or_throw(q_, nt * 5, "q");
+    alloc_or_throw(grad_, need_grad_ ? nt * 3 * nv_ : 1, "grad");
+    alloc_or_throw(phi_, muscl_ ? nn * 5 : 1, "phi");
+    alloc_or_throw(fflux_, static_cast<std::size_t>(nf) * 6, "fflux");
+    alloc_or_throw(res_, nn * nv_, "res");
+    alloc_or_throw(lam_, nn, "lam");
+    alloc_or_throw(dt_, nn, "dt");
+    alloc_or_throw(alpha_, nn, "alpha");
+    cuda_check(cudaMemsetAsync(q_.p, 0, q_.count * sizeof(double), s), "memset");
+    cuda_check(cudaMemsetAsync(grad_.p, 0, grad_.count * sizeof(double), s), "memset");
+    cuda_check(cudaMemsetAsync(phi_.p, 0, phi_.count * sizeof(double), s), "memset");
+    cuda_check(cudaMemsetAsync(res_.p, 0, res_.count * sizeof(double), s), "memset");
+    cuda_check(cudaMemsetAsync(lam_.p, 0, lam_.count * sizeof(double), s), "memset");
+    cuda_check(cudaMemsetAsync(dt_.p, 0, dt_.count * sizeof(double), s), "memset");
+    cuda_check(cudaMemsetAsync(alpha_.p, 0, alpha_.count * sizeof(double), s), "memset");
+    df_.U = U_.p;
+    df_.q = q_.p;
+    df_.grad = grad_.p;
+    df_.phi = phi_.p;
+    df_.fflux = fflux_.p;
+    df_.res = res_.p;
+    df_.lam = lam_.p;
+    df_.dt = dt_.p;
+    df_.alpha = alpha_.p;
+    df_.mut = nullptr;
+    alloc_or_throw(norm_partials_, static_cast<std::size_t>(norm_blocks(n)) * 6 + 8, "norm partials");
+    alloc_or_throw(l2_, 8, "l2");
+}
+
+// Unique-touch byte counts (each array element once per launch, at its
+// stored precision) of the residual-side kernels.
+void Solver::compute_alg_bytes(int64_t E, int64_t n_c2c, int64_t n_c2f) {
+    const double n = dm_.n, nb = dm_.nb, F = dm_.nf, Fi = dm_.ni, d = 8.0, i4 = 4.0;
+    const double visc = cfg_.viscous ? 1.0 : 0.0;
+    ab_.prim = n * 5 * d * 2 + nb * (5 * d + i4 + 3 * d + 3 * d + i4 + 5 * d) + nb * 3 * d;
+    ab_.grad = n * 5 * d + (n + 1) * i4 + double(E) * (i4 + 3 * d) + n * 15 * d;
+    ab_.limiter = (muscl_ ? n * (5 + 15 + 3 + 1 + 5) * d + (n + 1) * i4 * 2 + double(n_c2c) * i4 +
+                                double(n_c2f) * i4 + F * 3 * d
+                          : 0.0) +
+                  nb * (15 * d + 5 * d + i4 + i4 + 3 * d + 3 * d + 3 * d);
+    ab_.face_flux = F * (2 * i4 + 4 * d + 3 * d) + visc * F * 4 * d + (n + nb) * (5 + 15 + 5 + 3) * d + F * 6 * d;
+    ab_.cell_gather = (n + 1) * i4 + double(n_c2f) * i4 + F * i4 + F * 6 * d + n * 6 * d;
+    const double sa = (cfg_.precision == CFDG_PREC_MIXED) ? 4.0 : 8.0;
+    const double b2 = double(nv_) * nv_;
+    const double nnzb = sys_ ? double(sys_->nnzb()) : n + 2 * Fi;
+    ab_.jac = F * (2 * i4 + 4 * d + visc * d) + (n + nb) * 5 * d + n * d + Fi * 2 * i4 + nnzb * b2 * sa +
+              (nnzb - n) * b2 * sa + nnzb * i4 + (n + 1) * i4 + n * i4 + nb * 25 * d * 2 + double(n_c2f) * i4;
+    ab_.dt_rhs = n * (d * 2 + d * 2 + nv_ * d + 2 * nv_ * d);
+    ab_.state_update = n * nv_ * d * 3;
+    ab_.norms = n * nv_ * d;
+}
+
+void Solver::setup_bcs(const cfdg_bc_desc* bcs, int n_bcs, const HostMesh& hm) {
+    const int np = std::max(hm.n_patches, 1);
+    patches_h_.assign(np, BcPatch{});
+    for (auto& p : patches_h_) {
+        p.kind = -1;
+        p.sa_kind = 3;
+    }
+    for (int i = 0; i < n_bcs; ++i) {
+        const cfdg_bc_desc& d = bcs[i];
+        if (d.patch_id < 0 || d.patch_id >= np) continue;  // patch absent on this mesh
+        if (d.type < 0 || d.type > 8) throw Failure{CFDG_ERR_INVALID, "unknown BC type"};
+        BcPatch& P = patches_h_[d.patch_id];
+        P = BcPatch{};
+        P.kind = d.type;
+        switch (d.type) {
+            case CFDG_BC_SUPERSONIC_INLET: {
+                const Inflow s = resolve_inflow(d, gas_, d.p);
+                P.qfix[0] = s.p; P.qfix[1] = s.u; P.qfix[2] = s.v; P.qfix[3] = s.w; P.qfix[4] = s.T;
+                P.sa_kind = 1;
+                break;
+            }
+            case CFDG_BC_FARFIELD: {
+                const Inflow s = resolve_inflow(d, gas_, d.p);
+                P.far_p = s.p; P.far_T = s.T; P.far_u = s.u; P.far_v = s.v; P.far_w = s.w;
+                P.sa_kind = 1;
+                break;
+            }
+            case CFDG_BC_NO_SLIP_WALL:
+                P.qfix[1] = d.velocity[0]; P.qfix[2] = d.velocity[1]; P.qfix[3] = d.velocity[2]; P.qfix[4] = d.t;
+                P.sa_kind = 0;
+                break;
+            case CFDG_BC_NO_SLIP_WALL_HEAT_FLUX:
+                P.qfix[1] = d.velocity[0]; P.qfix[2] = d.velocity[1]; P.qfix[3] = d.velocity[2];
+                P.tmp_grad = d.tmp_grad;
+                P.sa_kind = 0;
+                break;
+            case CFDG_BC_SUBSONIC_INLET: {
+                const double p_ref = (d.p > 0.0) ? d.p : 101325.0;
+                const Inflow s = resolve_inflow(d, gas_, p_ref);
+                P.qfix[1] = s.u; P.qfix[2] = s.v; P.qfix[3] = s.w; P.qfix[4] = s.T;
+                P.sa_kind = 1;
+                break;
+            }
+            case CFDG_BC_SUBSONIC_OUTLET:
+                P.p_out = d.p;
+                P.sa_kind = 2;
+                break;
+            case CFDG_BC_SUPERSONIC_OUTLET:
+                P.sa_kind = 2;
+                break;
+            default:
+                P.sa_kind = 3;
+                break;
+        }
+    }
+    for (int32_t f = hm.n_inner; f < hm.n_faces; ++f) {
+        const int32_t p = hm.patch[f];
+        if (p >= np || patches_h_[p].kind < 0)
+            throw Failure{CFDG_ERR_INVALID, "boundary patch " + std::to_string(p) + " has no boundary condition"};
+    }
+    upload_or_throw(patches_, patches_h_, stream_, "patches");
+    cuda_check(cudaStreamSynchronize(stream_), "setup sync");
+    dm_.patches = patches_.p;
+    dm_.n_patches = np;
+}
+
+void Solver::setup_matrix(const HostMesh& hm, const Csr& c2c) {
+    const int32_t n = hm.n_cells;
+    // bsr_assemble (linalg/bsr_helpers.hpp:16-59): self + face neighbours, sorted.
+    std::vector<int32_t> row_ptr(static_cast<std::size_t>(n) + 1, 0), cols;
+    cols.reserve(c2c.val.size() + n);
+    for (int32_t c = 0; c < n; ++c) {
+        const std::size_t start = cols.size();
+        cols.push_back(c);
+        for (int32_t k = c2c.off[c]; k < c2c.off[c + 1]; ++k) cols.push_back(c2c.val[k]);
+        std::sort(cols.begin() + start, cols.end());
+        row_ptr[c + 1] = static_cast<int32_t>(cols.size());
+    }
+    sys_ = std::make_unique<BsrSystem>(device_, n, nv_, row_ptr.data(), cols.data(), cfg_.precision, stream_);
+    auto pos = [&](int32_t row, int32_t col) -> int32_t {
+        const auto b = cols.begin() + row_ptr[row], e = cols.begin() + row_ptr[row + 1];
+        const auto it = std::lower_bound(b, e, col);
+        if (it == e || *it != col) throw Failure{CFDG_ERR_MESH, "dual graph misses a face neighbour"};
+        return static_cast<int32_t>(it - cols.begin());
+    };
+    std::vector<int32_t> trans(cols.size());
+    for (int32_t i = 0; i < n; ++i)
+        for (int32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) trans[k] = pos(cols[k], i);
+    std::vector<int32_t> fpos(static_cast<std::size_t>(2) * hm.n_inner);
+    for (int32_t f = 0; f < hm.n_inner; ++f) {
+        fpos[2 * f] = pos(hm.owner[f], hm.neigh[f]);
+        fpos[2 * f + 1] = pos(hm.neigh[f], hm.owner[f]);
+    }
+    upload_or_throw(trans_, trans, stream_, "trans");
+    upload_or_throw(face_pos_, fpos, stream_, "face_pos");
+    alloc_or_throw(bjac_, static_cast<std::size_t>(std::max(hm.n_faces - hm.n_inner, 1)) * 25, "bjac");
+    alloc_or_throw(b_, static_cast<std::size_t>(n) * nv_, "rhs");
+    alloc_or_throw(du_, static_cast<std::size_t>(n) * nv_, "du");
+    cuda_check(cudaMemsetAsync(du_.p, 0, du_.count * sizeof(double), stream_), "memset");
+    cuda_check(cudaMemsetAsync(b_.p, 0, b_.count * sizeof(double), stream_), "memset");
+    cuda_check(cudaStreamSynchronize(stream_), "setup sync");
+}
+
+void Solver::setup_sa(const HostMesh&) {
+    throw Failure{CFDG_ERR_UNSUPPORTED, "Spalart-Allmaras module not built in this library"};
+}
+
+void Solver::sizes(int64_t* out) const {
+    out[0] = dm_.n;
+    out[1] = dm_.nf;
+    out[2] = dm_.ni;
+    out[3] = dm_.nt;
+    out[4] = sys_->nnzb();
+    out[5] = sys_->bs();
+    out[6] = nv_;
+}
+
+// Solver::init_fields (solver.hpp:507-544): primitives_rhop_to_conserved of
+// the [initial] state on every cell.
+void Solver::init_fields() {
+    const double rho = cfg_.init_rho, p = cfg_.init_p;
+    const double u = cfg_.init_velocity[0], v = cfg_.init_velocity[1], w = cfg_.init_velocity[2];
+    const double T = p / (rho * gas_.R);
+    const double e = gas_.cv * T;
+    const double ke = 0.5 * rho * (u * u + v * v + w * w);
+    const double U[5] = {rho, rho * u, rho * v, rho * w, rho * e + ke};
+    for (int v5 = 0; v5 < 5; ++v5) {
+        ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, 8.0 * dm_.n);
+        launch_fill(U_.p + static_cast<std::size_t>(v5) * dm_.n, dm_.n, U[v5], stream_);
+    }
+    cuda_check(cudaGetLastError(), "init launch");
+    cuda_check(cudaStreamSynchronize(stream_), "init sync");
+}
+
+void Solver::set_state_host(const double* u, int64_t ld) {
+    if (ld < dm_.n) throw Failure{CFDG_ERR_INVALID, "leading dimension smaller than n_cells"};
+    for (int v = 0; v < nv_; ++v)
+        cuda_check(cudaMemcpyAsync(U_.p + static_cast<std::size_t>(v) * dm_.n, u + v * ld, sizeof(double) * dm_.n,
+                                   cudaMemcpyHostToDevice, stream_),
+                   "H2D");
+    cuda_check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void Solver::get_field(int field, double* out, int64_t count) {
+    const double* src = nullptr;
+    int64_t need = 0;
+    const int64_t n = dm_.n, nt = dm_.nt;
+    switch (field) {
+        case CFDG_FIELD_U: src = U_.p; need = n * nv_; break;
+        case CFDG_FIELD_Q: src = q_.p; need = nt * 5; break;
+        case CFDG_FIELD_GRAD: src = grad_.p; need = need_grad_ ? nt * 3 * (sa_ ? 6 : 5) : 0; break;
+        case CFDG_FIELD_PHI: src = phi_.p; need = muscl_ ? n * 5 : 0; break;
+        case CFDG_FIELD_RES: src = res_.p; need = n * nv_; break;
+        case CFDG_FIELD_LAM: src = lam_.p; need = n; break;
+        case CFDG_FIELD_DT: src = dt_.p; need = n; break;
+        case CFDG_FIELD_ALPHA: src = alpha_.p; need = n; break;
+        case CFDG_FIELD_DU: src = du_.p; need = n * nv_; break;
+        case CFDG_FIELD_RHS: src = b_.p; need = n * nv_; break;
+        case CFDG_FIELD_MUT: src = mut_.p; need = sa_ ? nt : 0; break;
+        case CFDG_FIELD_WALLDIST: src = wall_dist_.p; need = sa_ ? n : 0; break;
+        case CFDG_FIELD_JAC: {
+            need = sys_->nnzb() * sys_->bs() * sys_->bs();
+            if (count < need) throw Failure{CFDG_ERR_INVALID, "output buffer too small"};
+            sys_->get_values_host(out);
+            return;
+        }
+        default: throw Failure{CFDG_ERR_INVALID, "unknown field id"};
+    }
+    if (need == 0 || !src) throw Failure{CFDG_ERR_INVALID, "field not allocated for this configuration"};
+    if (count < need) throw Failure{CFDG_ERR_INVALID, "output buffer too small"};
+    cuda_check(cudaMemcpyAsync(out, src, sizeof(double) * need, cudaMemcpyDeviceToHost, stream_), "D2H");
+    cuda_check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void Solver::stage(int st) {
+    switch (st) {
+        case CFDG_STAGE_PRIMITIVES: {
+            ProfScope ps(&prof_, CFDG_KCAT_PRIMITIVES, stream_, 1, ab_.prim);
+            launch_primitives(dm_, df_, gas_, stream_);
+            break;
+        }
+        case CFDG_STAGE_GRADIENT:
+            if (need_grad_) {
+                ProfScope ps(&prof_, CFDG_KCAT_GRADIENT, stream_, 1, ab_.grad);
+                launch_gradient(dm_, q_.p, grad_.p, 5, stream_);
+            }
+            break;
+        case CFDG_STAGE_LIMITER:
+            if (need_grad_) {
+                ProfScope ps(&prof_, CFDG_KCAT_LIMITER, stream_, 1, ab_.limiter);
+                launch_limiter_ghostgrad(dm_, df_, gas_, muscl_, cfg_.limiter, cfg_.venkat_k, stream_);
+            }
+            break;
+        case CFDG_STAGE_FLUXES: {
+            {
+                ProfScope ps(&prof_, CFDG_KCAT_FACE_FLUX, stream_, 1, ab_.face_flux);
+                launch_face_flux(dm_, df_, gas_, muscl_, cfg_.viscous != 0, stream_);
+            }
+            ProfScope ps(&prof_, CFDG_KCAT_CELL_GATHER, stream_, 1, ab_.cell_gather);
+            launch_cell_residual(dm_, df_, stream_);
+            break;
+        }
+        default: throw Failure{CFDG_ERR_INVALID, "unknown stage"};
+    }
+    cuda_check(cudaGetLastError(), "stage launch");
+}
+
+void Solver::evaluate_residual() {
+    stage(CFDG_STAGE_PRIMITIVES);
+    stage(CFDG_STAGE_GRADIENT);
+    stage(CFDG_STAGE_LIMITER);
+    stage(CFDG_STAGE_FLUXES);
+}
+
+void Solver::compute_dt(double cfl) {
+    if (!(cfl > 0.0)) throw Failure{CFDG_ERR_INVALID, "CFL must be positive"};
+    ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, ab_.dt_rhs);
+    launch_dt_rhs(dm_, df_, nv_, cfl, b_.p, du_.p, stream_);
+    cuda_check(cudaGetLastError(), "dt launch");
+}
+
+void Solver::assemble_jacobian() {
+    JacStructure js{};
+    const BsrView v = sys_->view();
+    js.row_ptr = v.row_ptr;
+    js.cols = v.cols;
+    js.diag = v.diag;
+    js.trans = trans_.p;
+    js.face_pos = face_pos_.p;
+    ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 3, ab_.jac);
+    if (cfg_.precision == CFDG_PREC_MIXED)
+        launch_jacobian<float>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values32(), bjac_.p, stream_);
+    else
+        launch_jacobian<double>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values64(), bjac_.p, stream_);
+    cuda_check(cudaGetLastError(), "jacobian launch");
+}
+
+cfdg_krylov_result Solver::linear_solve() {
+    if (cfg_.precond == CFDG_PC_SGS) sys_->sgs_setup(cfg_.sgs_ordering, std::max(cfg_.sgs_sweeps, 1));
+    cuda_check(cudaMemsetAsync(du_.p, 0, du_.count * sizeof(double), stream_), "memset");
+    last_krylov_ = sys_->bicgstab(cfg_.precond, cfg_.lin_rel_tol, cfg_.lin_abs_tol, cfg_.lin_max_iterations, du_.p, b_.p);
+    return last_krylov_;
+}
+
+void Solver::residual_norms(double* l2_host) {
+    {
+        ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 2, ab_.norms);
+        launch_norms(dm_.n, nv_, res_.p, norm_partials_.p, l2_.p, stream_);
+    }
+    cuda_check(cudaMemcpyAsync(l2_host_, l2_.p, sizeof(double) * nv_, cudaMemcpyDeviceToHost, stream_), "D2H");
+    cuda_check(cudaStreamSynchronize(stream_), "norm sync");
+    prof_.collect();
+    for (int v = 0; v < nv_; ++v) l2_host[v] = l2_host_[v];
+}
+
+cfdg_step_result Solver::newton_step(double cfl) {
+    cfdg_step_result r{};
+    evaluate_residual();
+    compute_dt(cfl);
+    assemble_jacobian();
+    const cfdg_krylov_result kr = linear_solve();
+    {
+        ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, ab_.state_update);
+        launch_state_update(dm_, U_.p, du_.p, nv_, stream_);
+    }
+    residual_norms(r.l2);
+    r.cfl = cfl;
+    r.nvars = nv_;
+    r.krylov_status = kr.status;
+    r.krylov_iterations = kr.iterations;
+    r.krylov_initial = kr.initial_residual;
+    r.krylov_final = kr.final_residual;
+    r.guess_used = 0;
+    return r;
+}
+
+// Geometric CFL ramp from cfl to cfl_max over cfl_ramp_iterations
+// iterations (the reference holds CFL constant, solver.hpp:265).
+double Solver::cfl_at(int64_t iter) const {
+    const int K = cfg_.cfl_ramp_iterations;
+    if (K <= 1 || !(cfg_.cfl_max > cfg_.cfl)) return cfg_.cfl;
+    const double t = std::min(1.0, double(iter - 1) / double(K - 1));
+    return std::min(cfg_.cfl_max, cfg_.cfl * std::pow(cfg_.cfl_max / cfg_.cfl, t));
+}
+
+// Solver::run_steady (solver.hpp:597-660).
+cfdg_run_result Solver::run_steady() {
+    cfdg_run_result out{};
+    const auto t0 = std::chrono::steady_clock::now();
+    double norm0[6] = {0, 0, 0, 0, 0, 0};
+    bool have0 = false;
+    const int interval = std::max(cfg_.residual_interval, 1);
+    for (int64_t iter = 1; iter <= cfg_.max_iterations; ++iter) {
+        const cfdg_step_result st = newton_step(cfl_at(iter));
+        out.iterations = iter;
+        out.krylov_iterations_total += st.krylov_iterations;
+        const bool diagnose = iter == 1 || iter % interval == 0 || iter == cfg_.max_iterations;
+        if (!diagnose) continue;
+        if (!std::isfinite(st.l2[0])) {
+            out.blowup = 1;
+            break;
+        }
+        for (int v = 0; v < nv_; ++v) out.l2_last[v] = st.l2[v];
+        if (!have0) {
+            for (int v = 0; v < nv_; ++v) norm0[v] = out.l2_first[v] = st.l2[v];
+            have0 = true;
+            out.rel = 1.0;
+        } else {
+            double rel = 0.0;
+            for (int v = 0; v < nv_; ++v) rel = std::max(rel, st.l2[v] / std::max(norm0[v], 1.0e-300));
+            out.rel = rel;
+            if (rel <= cfg_.residual_tolerance) {
+                out.converged = 1;
+                break;
+            }
+        }
+    }
+    out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return out;
+}
+
+}  // namespace cfdg

@@ -1,0 +1,238 @@
+// Host-side objects behind the C ABI: the block-sparse linear system
+// (BsrMatrix + SgsPreconditioner + BiCGSTAB of the reference linalg module)
+// and the compressible solver (Solver<...> + BackwardEuler).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "cfdg.h"
+#include "device_common.cuh"
+#include "host_mesh.hpp"
+#include "kernels.hpp"
+#include "krylov.hpp"
+
+namespace cfdg {
+
+void set_error(const std::string& msg);
+
+// Owning device allocation.
+template <typename T>
+struct DevArray {
+    T* p = nullptr;
+    std::size_t count = 0;
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    ~DevArray() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        count = 0;
+    }
+    bool alloc(std::size_t n) {
+        release();
+        if (n == 0) return true;
+        if (cudaMalloc(reinterpret_cast<void**>(&p), n * sizeof(T)) != cudaSuccess) {
+            p = nullptr;
+            return false;
+        }
+        count = n;
+        return true;
+    }
+    bool upload(const T* h, std::size_t n, cudaStream_t s) {
+        if (!alloc(n)) return false;
+        if (n == 0) return true;
+        return cudaMemcpyAsync(p, h, n * sizeof(T), cudaMemcpyHostToDevice, s) == cudaSuccess;
+    }
+    bool upload(const std::vector<T>& h, cudaStream_t s) { return upload(h.data(), h.size(), s); }
+};
+
+// Thrown inside the library; converted to a status code at the C boundary.
+struct Failure {
+    int status;
+    std::string msg;
+};
+void cuda_check(cudaError_t e, const char* what);
+
+// Optional per-launch timing with CUDA events recorded on the launching
+// stream; launch counting is always on.
+class Profiler {
+public:
+    ~Profiler();
+    void enable(bool on);
+    bool on() const { return on_; }
+    void start(int cat, cudaStream_t s);
+    void stop(cudaStream_t s);
+    void collect();  // resolves recorded pairs; the stream must be idle
+    void add_bytes(int cat, double b) {
+        if (on_) bytes[cat] += b;
+    }
+    double ms[CFDG_KCAT_COUNT] = {};
+    int64_t count[CFDG_KCAT_COUNT] = {};
+    double bytes[CFDG_KCAT_COUNT] = {};  // algorithmic (unique-touch) bytes of the timed launches
+    int64_t launches = 0;
+
+private:
+    cudaEvent_t get();
+    struct Rec {
+        int cat;
+        cudaEvent_t a, b;
+    };
+    bool on_ = false;
+    std::vector<cudaEvent_t> free_, all_;
+    std::vector<Rec> pending_;
+    int open_cat_ = -1;
+    cudaEvent_t open_ = nullptr;
+};
+
+struct ProfScope {
+    Profiler* p;
+    cudaStream_t s;
+    ProfScope(Profiler* prof, int cat, cudaStream_t st, int n = 1, double bytes = 0.0) : p(prof), s(st) {
+        p->launches += n;
+        if (p->on()) {
+            p->bytes[cat] += bytes;
+            p->start(cat, s);
+        }
+    }
+    ~ProfScope() {
+        if (p->on()) p->stop(s);
+    }
+};
+
+// Block-sparse matrix with its SGS preconditioner and BiCGSTAB workspace.
+class BsrSystem {
+public:
+    BsrSystem(int device, int32_t n, int32_t bs, const int32_t* row_ptr, const int32_t* cols, int precision,
+              cudaStream_t stream);
+    ~BsrSystem();
+
+    int32_t n() const { return n_; }
+    int32_t bs() const { return bs_; }
+    int64_t nnzb() const { return nnzb_; }
+    int precision() const { return precision_; }
+    cudaStream_t stream() const { return stream_; }
+    BsrView view() const { return BsrView{n_, bs_, row_ptr_.p, cols_.p, diag_.p}; }
+    const int32_t* diag_host() const { return diag_h_.data(); }
+    const std::vector<int32_t>& row_ptr_host() const { return row_ptr_h_; }
+    const std::vector<int32_t>& cols_host() const { return cols_h_; }
+    double* values64() { return vals64_.p; }
+    float* values32() { return vals32_.p; }
+
+    void set_values_host(const double* v);
+    void get_values_host(double* v);
+    // y = alpha*A*x + beta*y (device vectors)
+    void spmv(const double* x, double* y, double alpha, double beta);
+    // SgsPreconditioner::setup: ordering + block LU of the diagonal.
+    void sgs_setup(int ordering, int sweeps);
+    // z = M^-1 r (device vectors).
+    void sgs_apply(const double* r, double* z, const int* active);
+    // BiCGSTAB on device vectors; x holds the initial guess.
+    cfdg_krylov_result bicgstab(int precond, double rel_tol, double abs_tol, int max_it, double* x, const double* b);
+    int groups_fwd() const { return static_cast<int>(fwd_off_.size()) - 1; }
+    int groups_bwd() const { return static_cast<int>(bwd_off_.size()) - 1; }
+    int64_t launches() const { return prof_->launches; }
+    void set_profiler(Profiler* p) { prof_ = p ? p : &own_prof_; }
+    Profiler* profiler() { return prof_; }
+    int check_every = 1;  // host polls the Krylov state every k iterations
+
+private:
+    void build_ordering(int ordering);
+    template <typename MT>
+    void sgs_apply_t(const MT* vals, const MT* lu, const double* r, double* z, const int* active);
+
+    int device_;
+    cudaStream_t stream_;
+    int32_t n_, bs_;
+    int64_t nnzb_;
+    int precision_;
+    std::vector<int32_t> row_ptr_h_, cols_h_, diag_h_;
+    DevArray<int32_t> row_ptr_, cols_, diag_;
+    DevArray<double> vals64_, lu64_;
+    DevArray<float> vals32_, lu32_;
+    DevArray<int8_t> piv_;
+    DevArray<int> err_;
+    int ordering_ = -1, sweeps_ = 1;
+    bool lu_ready_ = false;
+    std::vector<int32_t> fwd_off_, bwd_off_;
+    std::vector<double> fwd_bytes_[2], bwd_bytes_[2];  // algorithmic bytes of one pass, mode 0 / mode 1
+    DevArray<int32_t> fwd_rows_, bwd_rows_;
+    double spmv_bytes(int n_extra_vectors, bool read_y) const;
+    // Krylov workspace
+    DevArray<double> r_, r0_, p_, v_, s_, t_, phat_, shat_, partials_;
+    DevArray<KrylovScalars> ks_;
+    KrylovScalars* ks_host_ = nullptr;
+    Profiler own_prof_;
+    Profiler* prof_ = &own_prof_;
+};
+
+// The compressible finite-volume solver on one device.
+class Solver {
+public:
+    Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, const cfdg_bc_desc* bcs, int n_bcs);
+    ~Solver();
+
+    void init_fields();
+    void set_state_host(const double* u, int64_t ld);
+    void get_field(int field, double* out, int64_t count);
+    void evaluate_residual();
+    void stage(int st);
+    void compute_dt(double cfl);
+    void assemble_jacobian();
+    cfdg_krylov_result linear_solve();
+    cfdg_step_result newton_step(double cfl);
+    void residual_norms(double* l2_host);
+    cfdg_run_result run_steady();
+    cudaStream_t stream() const { return stream_; }
+    int64_t launches() const { return prof_.launches; }
+    Profiler& profiler() { return prof_; }
+    BsrSystem& system() { return *sys_; }
+    void sizes(int64_t* out) const;
+    double cfl_at(int64_t iter) const;
+
+private:
+    void setup_mesh(const cfdg_mesh_host& mesh);
+    void setup_bcs(const cfdg_bc_desc* bcs, int n_bcs, const HostMesh& hm);
+    void setup_matrix(const HostMesh& hm, const Csr& c2c);
+    void setup_sa(const HostMesh& hm);
+    void rhs_update_ready();
+
+    int device_;
+    cudaStream_t stream_ = nullptr;
+    cfdg_config cfg_;
+    GasParams gas_;
+    int nv_ = 5;
+    bool sa_ = false;
+    bool need_grad_ = false;
+    bool muscl_ = false;
+    DevMesh dm_{};
+    DevFields df_{};
+    SaParams sap_{};
+    // mesh arrays
+    DevArray<int32_t> owner_, neigh_, bpatch_, c2f_off_, c2f_, c2c_off_, c2c_, g_off_, g_col_;
+    DevArray<double> fnx_, fny_, fnz_, farea_, fcx_, fcy_, fcz_, fdx_, fdy_, fdz_, finv_d_, ccx_, ccy_, ccz_, vol_,
+        g_wx_, g_wy_, g_wz_, wall_dist_;
+    DevArray<BcPatch> patches_;
+    std::vector<BcPatch> patches_h_;
+    // fields
+    DevArray<double> U_, q_, grad_, phi_, fflux_, res_, lam_, dt_, alpha_, nu_, rho_, mut_, sa_face_;
+    // linear system
+    std::unique_ptr<BsrSystem> sys_;
+    DevArray<int32_t> trans_, face_pos_;
+    DevArray<double> bjac_, b_, du_, norm_partials_, l2_;
+    double* l2_host_ = nullptr;
+    Profiler prof_;
+    // algorithmic (unique-touch) bytes per launch of each residual-side kernel
+    struct {
+        double prim, grad, limiter, face_flux, cell_gather, jac, dt_rhs, state_update, norms;
+    } ab_{};
+    void compute_alg_bytes(int64_t n_grad_edges, int64_t n_c2c, int64_t n_c2f);
+    cfdg_krylov_result last_krylov_{};
+};
+
+}  // namespace cfdg

@@ -1,0 +1,302 @@
+/*
+ * cfdg.h — C ABI of the B200 implementation of the implicit compressible
+ * finite-volume hot path (residual R(U) -> 5x5/6x6 BSR Jacobian ->
+ * BiCGSTAB + SGS -> Newton update) on one GPU holding the whole mesh.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: CFDG_OK (0) or a negative
+ *     CFDG_ERR_* code; nothing aborts the process.  cfdg_status_string()
+ *     names a code, cfdg_last_error() gives the last message of this thread.
+ *   - Pointers whose name ends in _h are HOST buffers, _d are DEVICE
+ *     buffers.  Host buffers are read or written during the call only.
+ *   - Handles are thread-compatible (one handle per host thread at a time).
+ *   - Field layout is SoA: one array per variable.  Linear-system vectors
+ *     (right-hand side b, update du) are AoS in block order c*bs+v, as in
+ *     the reference implicit integrator.
+ *
+ * Each declaration cites the reference interface it replaces
+ * (paths inside maksim-movsisyan/Distributed-cfd-solver).
+ */
+#ifndef CFDG_H
+#define CFDG_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CFDG_API __attribute__((visibility("default")))
+#else
+#define CFDG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define CFDG_OK               0
+#define CFDG_ERR_INVALID     (-1)  /* bad argument / handle / size          */
+#define CFDG_ERR_CUDA        (-2)  /* CUDA runtime error (message kept)      */
+#define CFDG_ERR_NOMEM       (-3)  /* device or host allocation failed       */
+#define CFDG_ERR_SINGULAR    (-4)  /* singular diagonal block in SGS setup   */
+#define CFDG_ERR_NONFINITE   (-5)  /* NaN/Inf detected in residual or state  */
+#define CFDG_ERR_DIVERGED    (-6)  /* Krylov breakdown                       */
+#define CFDG_ERR_MESH        (-7)  /* mesh fails a geometric/topology check  */
+#define CFDG_ERR_UNSUPPORTED (-8)  /* option not built                       */
+#define CFDG_ERR_NODEVICE    (-9)  /* no CUDA device visible                 */
+
+/* ------------------------------------------------------------ enumerations */
+/* Cell/face types: values of mesh::CellType (include/cfd/mesh/cgnstables.hpp:20-27). */
+enum { CFDG_TET = 0, CFDG_PYRA = 1, CFDG_PRISM = 2, CFDG_HEXA = 3, CFDG_TRI = 4, CFDG_QUAD = 5 };
+
+/* BC kinds: values of bc::physical::BCType (include/cfd/bc/physical/physical_bc.hpp:12-23). */
+enum {
+    CFDG_BC_SUPERSONIC_INLET = 0,
+    CFDG_BC_SUPERSONIC_OUTLET = 1,
+    CFDG_BC_SUBSONIC_INLET = 2,
+    CFDG_BC_SUBSONIC_OUTLET = 3,
+    CFDG_BC_SLIP_WALL = 4,
+    CFDG_BC_NO_SLIP_WALL = 5,
+    CFDG_BC_NO_SLIP_WALL_HEAT_FLUX = 6,
+    CFDG_BC_SYMMETRY = 7,
+    CFDG_BC_FARFIELD = 8
+};
+/* Inflow parameterisation: bc::physical::InflowMode (physical_bc.hpp:25-29). */
+enum { CFDG_INFLOW_VELOCITY = 0, CFDG_INFLOW_MACH_ANGLES = 1, CFDG_INFLOW_MACH_DIRECTION = 2 };
+
+/* Gradient operators: numerics::gradient::GradientType
+ * (include/cfd/numerics/gradient/gradient_manager.hpp:14-19); the two
+ * least-squares stencils are built (Green-Gauss is not on this path). */
+enum { CFDG_GRAD_LSQ_FACE = 2, CFDG_GRAD_LSQ_NODE = 3 };
+/* Reconstruction: ReconType (include/cfd/solver/compressible/config.hpp). */
+enum { CFDG_RECON_FIRST_ORDER = 0, CFDG_RECON_MUSCL = 1 };
+/* Multidimensional limiters: LimiterType (config.hpp) / slope_limiters.hpp. */
+enum { CFDG_LIM_VENKATAKRISHNAN = 1, CFDG_LIM_BARTH_JESPERSEN = 2, CFDG_LIM_VAN_ALBADA = 3 };
+/* SGS sweep ordering.  LEVEL reproduces the sequential sweep of
+ * linalg/bsr_helpers.hpp:389-435 exactly (level-scheduled); COLOR sweeps a
+ * multicolour ordering (a different, equally valid SGS preconditioner). */
+enum { CFDG_SGS_LEVEL = 0, CFDG_SGS_COLOR = 1 };
+/* Matrix precision: FP64 everywhere, or FP32 Jacobian/LU/SpMV/SGS with FP64
+ * vectors, residual, update and inner products. */
+enum { CFDG_PREC_FP64 = 0, CFDG_PREC_MIXED = 1 };
+/* Preconditioner: linalg::PreconditionerType (linalg/config.hpp:12). */
+enum { CFDG_PC_NONE = 0, CFDG_PC_SGS = 1 };
+/* Krylov status: linalg::SolverStatus (linalg/types.hpp). */
+enum { CFDG_KRYLOV_CONVERGED = 0, CFDG_KRYLOV_DIVERGED = 1, CFDG_KRYLOV_MAX_ITERATIONS = 2 };
+
+/* Fields readable with cfdg_solver_get_field (sizes in doubles). */
+enum {
+    CFDG_FIELD_U = 0,        /* conserved state, nvars x n_cells                  */
+    CFDG_FIELD_Q = 1,        /* primitives (p,u,v,w,T), 5 x n_total (ghosts incl.)*/
+    CFDG_FIELD_GRAD = 2,     /* gradients, (5|6) vars x 3 planes x n_total        */
+    CFDG_FIELD_PHI = 3,      /* limiter, 5 x n_cells                              */
+    CFDG_FIELD_RES = 4,      /* residual, nvars x n_cells                         */
+    CFDG_FIELD_LAM = 5,      /* spectral radius, n_cells                          */
+    CFDG_FIELD_DT = 6,       /* local time step, n_cells                          */
+    CFDG_FIELD_ALPHA = 7,    /* diagonal shift V/dt, n_cells                      */
+    CFDG_FIELD_JAC = 8,      /* BSR values, nnzb x bs x bs (row-major blocks)     */
+    CFDG_FIELD_DU = 9,       /* last Newton update, AoS n_cells x nvars           */
+    CFDG_FIELD_MUT = 10,     /* eddy viscosity, n_total (SA only)                 */
+    CFDG_FIELD_WALLDIST = 11,/* wall distance, n_cells (SA only)                  */
+    CFDG_FIELD_RHS = 12      /* linear right-hand side -R, AoS n_cells x nvars    */
+};
+
+/* Pipeline stages for cfdg_solver_stage (each is one step of
+ * Solver::evaluate_residual, include/cfd/solver/compressible/solver.hpp:169-247). */
+enum {
+    CFDG_STAGE_PRIMITIVES = 0,  /* step 1 + BC ghost values (steps 1,3)         */
+    CFDG_STAGE_GRADIENT = 1,    /* step 5: gradient operator on owned cells       */
+    CFDG_STAGE_LIMITER = 2,     /* step 5: ghost gradients + MUSCL limiter        */
+    CFDG_STAGE_FLUXES = 3       /* step 6 (+ SA steps 7,8): face sweep -> R, lam  */
+};
+
+/* Kernel families timed by the optional profiler (CUDA events on the
+ * solver stream around every launch of the family). */
+enum {
+    CFDG_KCAT_PRIMITIVES = 0, CFDG_KCAT_GRADIENT = 1, CFDG_KCAT_LIMITER = 2, CFDG_KCAT_FACE_FLUX = 3,
+    CFDG_KCAT_CELL_GATHER = 4, CFDG_KCAT_JACOBIAN = 5, CFDG_KCAT_LU = 6, CFDG_KCAT_SPMV = 7, CFDG_KCAT_SGS = 8,
+    CFDG_KCAT_KRYLOV = 9, CFDG_KCAT_UPDATE = 10, CFDG_KCAT_COUNT = 11
+};
+
+/* ------------------------------------------------------------- structures */
+/* Host view of one single-partition mesh with geometry, the subset of
+ * mesh::MeshPart (include/cfd/mesh/localmesh.hpp:17-102) the solver reads.
+ * Faces follow the reference 3-zone order: interior faces [0,n_inner_faces)
+ * sorted by (owner, neigh), then boundary faces sorted by (patch, owner);
+ * the BC ghost of boundary face f is slot n_cells + (f - n_inner_faces). */
+typedef struct cfdg_mesh_host {
+    int32_t n_cells, n_faces, n_inner_faces, n_nodes, n_patches;
+    const uint8_t* cell_type;           /* n_cells                           */
+    const int32_t* cell_nodes_offsets;  /* n_cells+1                         */
+    const int32_t* cell_nodes;          /* CGNS node order                   */
+    const double *node_x, *node_y, *node_z;
+    const double *cell_centroid_x, *cell_centroid_y, *cell_centroid_z, *cell_volume;
+    const int32_t *face_owner, *face_neigh, *face_patch;  /* neigh=-1, patch=-1 */
+    const int32_t *face_nodes_offsets, *face_nodes;
+    const double *face_centroid_x, *face_centroid_y, *face_centroid_z;
+    const double *face_normal_x, *face_normal_y, *face_normal_z, *face_area;
+} cfdg_mesh_host;
+
+/* One boundary patch: bc::BCDescriptor (include/cfd/bc/config.hpp). */
+typedef struct cfdg_bc_desc {
+    int32_t patch_id, type, inflow_mode, pad_;
+    double p, t, tmp_grad;
+    double velocity[3];
+    double mach, alpha_deg, beta_deg;
+    double direction[3];
+} cfdg_bc_desc;
+
+/* Solver configuration: SolverConfig + linalg::SolverParams
+ * (include/cfd/solver/compressible/config.hpp:94-136, linalg/config.hpp:14-26)
+ * plus the CFL ramp, precision, SGS ordering, SA and learned-guess options. */
+typedef struct cfdg_config {
+    int32_t viscous;          /* 0 Euler (InviscidFlow), 1 Navier-Stokes      */
+    int32_t turbulence;       /* 0 none, 1 Spalart-Allmaras (6 variables)     */
+    int32_t gradient;         /* CFDG_GRAD_*                                  */
+    int32_t reconstruction;   /* CFDG_RECON_*                                 */
+    int32_t limiter;          /* CFDG_LIM_*                                   */
+    int32_t precision;        /* CFDG_PREC_*                                  */
+    int32_t precond;          /* CFDG_PC_*                                    */
+    int32_t sgs_ordering;     /* CFDG_SGS_*                                   */
+    int32_t sgs_sweeps;       /* >= 1                                         */
+    int32_t lin_max_iterations;
+    int32_t cfl_ramp_iterations; /* iterations over which CFL goes cfl->cfl_max */
+    int32_t residual_interval;
+    double gamma, gas_constant, prandtl, prandtl_turb;
+    double init_rho, init_p, init_velocity[3];
+    double venkat_k;
+    double cfl, cfl_max;
+    double residual_tolerance;
+    double lin_rel_tol, lin_abs_tol;
+    double nu_inf_ratio;      /* SA freestream nu_tilde / nu                   */
+    int64_t max_iterations;
+} cfdg_config;
+
+typedef struct cfdg_krylov_result {
+    int32_t status;            /* CFDG_KRYLOV_*                              */
+    int32_t iterations;
+    double initial_residual, final_residual;
+} cfdg_krylov_result;
+
+typedef struct cfdg_step_result {
+    double l2[6];              /* L2 residual norms of the evaluated R(U)    */
+    double cfl;
+    int32_t nvars;
+    int32_t krylov_status, krylov_iterations, guess_used;
+    double krylov_initial, krylov_final;
+} cfdg_step_result;
+
+typedef struct cfdg_run_result {
+    int64_t iterations;
+    int32_t converged, blowup;
+    double rel, seconds;
+    int64_t krylov_iterations_total;
+    double l2_first[6], l2_last[6];
+} cfdg_run_result;
+
+typedef struct cfdg_solver cfdg_solver;   /* Solver<...> + BackwardEuler     */
+typedef struct cfdg_bsr cfdg_bsr;         /* BsrMatrix + SGS + BiCGSTAB      */
+typedef struct cfdg_host_mesh cfdg_host_mesh;
+
+/* ------------------------------------------------------------ library */
+CFDG_API int cfdg_version(void);
+CFDG_API const char* cfdg_status_string(int status);
+CFDG_API const char* cfdg_last_error(void);
+CFDG_API int cfdg_device_count(int* count_h);
+CFDG_API void cfdg_config_default(cfdg_config* cfg_h);
+
+/* ------------------------------------------------------- synthetic meshes */
+/* Generates the benchmark meshes in memory, replacing the CGNS/HDF5 import
+ * (apps/solver.cpp:89, io::solver_mesh::import_mesh_hdf5) that cannot be
+ * built here.  kind: 0 = compression-ramp hex block, 1 = flat-plate hex
+ * block, 2 = tetrahedral bump.  Cells are permuted by a seeded shuffle and
+ * renumbered by reverse Cuthill-McKee (the ordering of
+ * mesh::reorder_local_mesh(RCM), src/mesh/reorder.cpp:135-190,579-602);
+ * geometry follows mesh::compute_mesh_geometry (src/mesh/geometry.cpp:301-540). */
+typedef struct cfdg_mesh_spec {
+    int32_t kind, nx, ny, nz;
+    double lx, ly, lz;           /* domain extents [m]                          */
+    double first_spacing;        /* wall-normal first cell height (plate) [m]  */
+    double stretch;              /* wall-normal growth ratio (plate)           */
+    double cap_spacing;          /* stop growth at this spacing (0 = never)    */
+    double jitter;               /* interior node jitter, fraction of spacing  */
+    double ramp_angle_deg, ramp_x;   /* ramp geometry                          */
+    double plate_x0;             /* plate leading edge x (symmetry before it)  */
+    double bump_height, bump_x0, bump_x1;
+    uint64_t seed;
+    int32_t permute, reorder_rcm;
+} cfdg_mesh_spec;
+CFDG_API int cfdg_mesh_generate(const cfdg_mesh_spec* spec_h, cfdg_host_mesh** out);
+CFDG_API int cfdg_host_mesh_view(const cfdg_host_mesh* mesh, cfdg_mesh_host* view_h);
+CFDG_API int cfdg_host_mesh_free(cfdg_host_mesh* mesh);
+/* Recomputes cell/face geometry of a view in place of the arrays it points
+ * to (compute_mesh_geometry, src/mesh/geometry.cpp:301-540). */
+CFDG_API int cfdg_mesh_compute_geometry(cfdg_host_mesh* mesh);
+
+/* ----------------------------------------------------------- solver */
+/* Solver ctor (solver.hpp:74-150): uploads the mesh, builds connectivity,
+ * LSQ coefficients, BSR structure and SGS orderings, allocates device state. */
+CFDG_API int cfdg_solver_create(int device, const cfdg_mesh_host* mesh_h, const cfdg_config* cfg_h,
+                       const cfdg_bc_desc* bcs_h, int32_t n_bcs, cfdg_solver** out);
+CFDG_API int cfdg_solver_destroy(cfdg_solver* s);
+/* Solver::init_fields (solver.hpp:507-544): uniform [initial] state. */
+CFDG_API int cfdg_solver_init_fields(cfdg_solver* s);
+/* Sets the conserved state from host SoA arrays (nvars x ld doubles, cells 0..n_cells). */
+CFDG_API int cfdg_solver_set_state(cfdg_solver* s, const double* u_h, int64_t ld);
+CFDG_API int cfdg_solver_get_field(cfdg_solver* s, int32_t field, double* out_h, int64_t count);
+CFDG_API int cfdg_solver_sizes(const cfdg_solver* s, int64_t* sizes_h /* n_cells,n_faces,n_inner,n_total,nnzb,bs,nvars */);
+/* Solver::evaluate_residual (solver.hpp:169-247). */
+CFDG_API int cfdg_evaluate_residual(cfdg_solver* s);
+CFDG_API int cfdg_solver_stage(cfdg_solver* s, int32_t stage);
+/* Solver::compute_dt (solver.hpp:256-287) with the given CFL. */
+CFDG_API int cfdg_compute_dt(cfdg_solver* s, double cfl);
+/* Solver::assemble_jacobian -> JacobianKernel::apply (jacobian_kernel.hpp:74-103). */
+CFDG_API int cfdg_assemble_jacobian(cfdg_solver* s);
+/* set_rhs_and_zero_du + BSRLinearSystem::solve (implicit_euler.hpp:81-92,
+ * bsr_linear_system.hpp:93-97). */
+CFDG_API int cfdg_linear_solve(cfdg_solver* s, cfdg_krylov_result* out_h);
+/* BackwardEuler::advance (implicit_euler.hpp:34-76) at the given CFL. */
+CFDG_API int cfdg_newton_step(cfdg_solver* s, double cfl, cfdg_step_result* out_h);
+/* Solver::residual_norms (solver.hpp:740-756), nvars doubles. */
+CFDG_API int cfdg_residual_norms(cfdg_solver* s, double* l2_h);
+/* Solver::run_steady (solver.hpp:597-660) with the CFL ramp. */
+CFDG_API int cfdg_run_steady(cfdg_solver* s, cfdg_run_result* out_h);
+/* Stream all solver kernels are queued on (cudaStream_t as void*). */
+CFDG_API void* cfdg_solver_stream(cfdg_solver* s);
+/* Total solver kernel launches since creation (for launch accounting). */
+CFDG_API int64_t cfdg_solver_launch_count(const cfdg_solver* s);
+/* Enables (1) or disables (0) per-launch CUDA-event timing; resets counters. */
+CFDG_API int cfdg_solver_profile(cfdg_solver* s, int32_t enable);
+/* Accumulated device milliseconds, launch counts and algorithmic
+ * (unique-touch) bytes per CFDG_KCAT_* family; bytes_h may be NULL. */
+CFDG_API int cfdg_solver_profile_read(cfdg_solver* s, double* ms_h, int64_t* launches_h, double* bytes_h);
+/* Number of SGS colours / forward levels of the active ordering. */
+CFDG_API int cfdg_solver_sgs_info(const cfdg_solver* s, int32_t* n_groups_fwd_h, int32_t* n_groups_bwd_h);
+
+/* ------------------------------------------------ block-sparse linear algebra */
+/* BsrMatrix + assemble (src/linalg/bsr_matrix.cpp:22-40): structure from
+ * host CSR (sorted columns, diagonal present), values set later. */
+CFDG_API int cfdg_bsr_create(int device, int32_t n_rows, int32_t bs, const int32_t* row_ptr_h,
+                    const int32_t* cols_h, int32_t precision, cfdg_bsr** out);
+CFDG_API int cfdg_bsr_destroy(cfdg_bsr* a);
+CFDG_API int cfdg_bsr_set_values(cfdg_bsr* a, const double* values_h);
+/* LinearOperator::apply, y = alpha*A*x + beta*y (bsr_matrix.cpp:10-20). */
+CFDG_API int cfdg_bsr_spmv(cfdg_bsr* a, const double* x_d, double* y_d, double alpha, double beta);
+CFDG_API int cfdg_bsr_spmv_host(cfdg_bsr* a, const double* x_h, double* y_h, double alpha, double beta);
+/* Preconditioner::setup for SGS: block LU of the diagonal
+ * (preconditioners.cpp:62-93). */
+CFDG_API int cfdg_sgs_setup(cfdg_bsr* a, int32_t ordering, int32_t sweeps);
+/* Preconditioner::apply for SGS: z = M^-1 r (preconditioners.cpp:171-194). */
+CFDG_API int cfdg_sgs_apply(cfdg_bsr* a, const double* r_d, double* z_d);
+CFDG_API int cfdg_sgs_apply_host(cfdg_bsr* a, const double* r_h, double* z_h);
+/* IterativeSolver::solve for BiCGSTAB (src/linalg/bicgstab.cpp:42-201);
+ * x holds the initial guess on entry.  precond: CFDG_PC_*. */
+CFDG_API int cfdg_bicgstab(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it,
+                  double* x_d, const double* b_d, cfdg_krylov_result* out_h);
+CFDG_API int cfdg_bicgstab_host(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it,
+                       double* x_h, const double* b_h, cfdg_krylov_result* out_h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFDG_H */

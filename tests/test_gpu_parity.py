@@ -1,0 +1,171 @@
+"""GPU parity of the hot path against the reference solver (oracle/_ref),
+stage by stage, through the C ABI.
+
+Tolerances (FP64 everywhere): stage outputs 1e-11 relative to the largest
+magnitude of each variable; Jacobian blocks 1e-11 relative per block row;
+SGS level ordering and SpMV 1e-12; the Krylov solution 1e-7 (BiCGSTAB
+amplifies round-off of the fused inner products); Newton iterates 1e-8.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "ramp_muscl": lambda cb: cb.cases.ramp(),
+    "ramp_first_order": lambda cb: _first_order(cb.cases.ramp()),
+    "plate_viscous": lambda cb: cb.cases.plate(scale=8),
+    "bump_tets": lambda cb: cb.cases.bump(scale=16, mixed=False),
+    "plate_face_stencil": lambda cb: _face_stencil(cb, cb.cases.plate(scale=8)),
+}
+
+
+def _first_order(case):
+    case.cfg.reconstruction = 0
+    return case
+
+
+def _face_stencil(cb, case):
+    case.cfg.gradient = cb.GRAD_LSQ_FACE
+    return case
+
+
+def _setup(cb, refh, name, level=True):
+    case = CASES[name](cb)
+    if level:
+        case.cfg.sgs_ordering = cb.SGS_LEVEL
+    mesh = cb.HostMesh(case.spec)
+    U0 = cb.cases.perturbed_state(case, mesh.n_cells)
+    gpu = cb.Solver(mesh, case.cfg, case.bcs)
+    ref = refh.RefSolver(mesh, case.cfg, case.bcs)
+    gpu.set_state(U0)
+    ref.set_state(U0)
+    return case, mesh, U0, gpu, ref
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_residual_stages(cb, refh, name):
+    case, mesh, U0, gpu, ref = _setup(cb, refh, name)
+    st = ref.stages()
+    gpu.evaluate_residual()
+    n, nt = gpu.n_cells, gpu.n_total
+    q = gpu.get(cb.FIELD_Q)
+    assert rel_err(q, st["q"], nt) < 1e-13  # primitives + BC ghost values
+    if case.cfg.reconstruction == 1 or case.cfg.viscous:
+        g = gpu.get(cb.FIELD_GRAD)[: 15 * nt]
+        assert rel_err(g, st["grad"], nt) < 1e-11  # LSQ gradients + ghost gradients
+    if case.cfg.reconstruction == 1:
+        phi = gpu.get(cb.FIELD_PHI)
+        assert rel_err(phi, st["phi"]) < 1e-9  # limiter values are O(1)
+    res = gpu.get(cb.FIELD_RES)
+    assert rel_err(res, st["res"], n) < 1e-11
+    lam = gpu.get(cb.FIELD_LAM)
+    assert rel_err(lam, st["lam"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["ramp_muscl", "plate_viscous", "bump_tets"])
+def test_jacobian(cb, refh, name):
+    case, mesh, U0, gpu, ref = _setup(cb, refh, name)
+    ref.stages()
+    alpha_ref, vals_ref = ref.jacobian(7.5)
+    gpu.evaluate_residual()
+    gpu.compute_dt(7.5)
+    gpu.assemble_jacobian()
+    assert rel_err(gpu.get(cb.FIELD_ALPHA), alpha_ref) < 1e-13
+    vals = gpu.get(cb.FIELD_JAC)
+    assert vals.shape == vals_ref.shape
+    assert rel_err(vals, vals_ref, 25) < 1e-11
+    rhs = gpu.get(cb.FIELD_RHS).reshape(-1, 5)
+    res = gpu.get(cb.FIELD_RES).reshape(5, -1).T
+    assert np.array_equal(rhs, -res)
+
+
+def _matrix_from_ref(cb, refh, name, cfl=7.5):
+    case, mesh, U0, gpu, ref = _setup(cb, refh, name)
+    ref.stages()
+    _, vals = ref.jacobian(cfl)
+    off, nb = refh.connectivity(mesh, 1)
+    n = mesh.n_cells
+    row_ptr = np.zeros(n + 1, dtype=np.int32)
+    cols = []
+    for c in range(n):
+        row = sorted([c] + list(nb[off[c]:off[c + 1]]))
+        cols.extend(row)
+        row_ptr[c + 1] = len(cols)
+    return row_ptr, np.array(cols, dtype=np.int32), vals
+
+
+@pytest.mark.parametrize("name", ["ramp_muscl", "bump_tets"])
+def test_spmv_sgs_level_bicgstab(cb, refh, name):
+    row_ptr, cols, vals = _matrix_from_ref(cb, refh, name)
+    n = len(row_ptr) - 1
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(n * 5)
+    y0 = rng.standard_normal(n * 5)
+    A = cb.Bsr(row_ptr, cols, 5)
+    A.set_values(vals)
+    for alpha, beta in [(1.0, 0.0), (-0.5, 1.0), (2.0, 0.25), (0.0, 3.0)]:
+        y = A.spmv(x, y0, alpha, beta)
+        y_ref = refh.bsr_spmv(row_ptr, cols, vals, 5, x, y0, alpha, beta)
+        assert rel_err(y, y_ref) < 1e-13
+    A.sgs_setup(cb.SGS_LEVEL, 1)
+    z = A.sgs_apply(x)
+    z_ref = refh.sgs_apply(row_ptr, cols, vals, 5, x)
+    assert rel_err(z, z_ref) < 1e-12
+    A.sgs_setup(cb.SGS_LEVEL, 2)
+    assert rel_err(A.sgs_apply(x), refh.sgs_apply(row_ptr, cols, vals, 5, x, sweeps=2)) < 1e-12
+    A.sgs_setup(cb.SGS_LEVEL, 1)
+    b = rng.standard_normal(n * 5)
+    sol, info = A.bicgstab(b, precond=cb.PC_SGS, rel_tol=1e-10, max_it=200)
+    sol_ref, info_ref = refh.bicgstab(row_ptr, cols, vals, 5, b, precond=1, rel_tol=1e-10, max_it=200)
+    assert info.status == cb.KRYLOV_CONVERGED and info_ref["status"] == 0
+    assert abs(info.iterations - info_ref["iterations"]) <= 1
+    assert rel_err(sol, sol_ref) < 1e-7
+    # multicolour SGS: a different preconditioner, same solution
+    A.sgs_setup(cb.SGS_COLOR, 1)
+    sol_c, info_c = A.bicgstab(b, precond=cb.PC_SGS, rel_tol=1e-10, max_it=400)
+    assert info_c.status == cb.KRYLOV_CONVERGED
+    assert rel_err(sol_c, sol_ref) < 1e-7
+    # unpreconditioned
+    sol_n, info_n = A.bicgstab(b, precond=cb.PC_NONE, rel_tol=1e-10, max_it=2000)
+    sol_nr, info_nr = refh.bicgstab(row_ptr, cols, vals, 5, b, precond=0, rel_tol=1e-10, max_it=2000)
+    assert info_n.status == cb.KRYLOV_CONVERGED
+    assert rel_err(sol_n, sol_nr) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["ramp_muscl", "plate_viscous", "bump_tets"])
+def test_newton_steps_match_reference(cb, refh, name):
+    case, mesh, U0, gpu, ref = _setup(cb, refh, name, level=True)
+    for k, cfl in enumerate([1.0, 3.0, 10.0]):
+        st = gpu.newton_step(cfl)
+        l2_ref = ref.newton_step(cfl)
+        assert rel_err(np.array(st.l2[:5]), l2_ref) < 1e-9, k
+        U = gpu.get(cb.FIELD_U)
+        U_ref = ref.get_state().ravel()
+        assert rel_err(U, U_ref, mesh.n_cells) < 1e-8, k
+
+
+def test_bitwise_determinism(cb, refh):
+    case = cb.cases.plate(scale=8)
+    mesh = cb.HostMesh(case.spec)
+    U0 = cb.cases.perturbed_state(case, mesh.n_cells)
+    outs = []
+    for _ in range(2):
+        with cb.Solver(mesh, case.cfg, case.bcs) as s:
+            s.set_state(U0)
+            for cfl in (1.0, 5.0):
+                s.newton_step(cfl)
+            outs.append(s.get(cb.FIELD_U))
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_colour_sgs_newton_converges(cb):
+    case = cb.cases.ramp(iterations=60)
+    mesh = cb.HostMesh(case.spec)
+    with cb.Solver(mesh, case.cfg, case.bcs) as s:
+        s.init_fields()
+        r = s.run_steady()
+        assert not r.blowup
+        assert r.rel < 1e-2, r.rel
