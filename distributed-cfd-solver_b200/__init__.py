@@ -77,7 +77,7 @@ class Config(C.Structure):
                 ("reconstruction", C.c_int32), ("limiter", C.c_int32), ("precision", C.c_int32),
                 ("precond", C.c_int32), ("sgs_ordering", C.c_int32), ("sgs_sweeps", C.c_int32),
                 ("lin_max_iterations", C.c_int32), ("cfl_ramp_iterations", C.c_int32),
-                ("residual_interval", C.c_int32),
+                ("residual_interval", C.c_int32), ("convergence_monitor", C.c_int32), ("reserved_", C.c_int32),
                 ("gamma", C.c_double), ("gas_constant", C.c_double), ("prandtl", C.c_double),
                 ("prandtl_turb", C.c_double), ("init_rho", C.c_double), ("init_p", C.c_double),
                 ("init_velocity", C.c_double * 3), ("venkat_k", C.c_double), ("cfl", C.c_double),

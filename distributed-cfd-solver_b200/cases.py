@@ -67,7 +67,7 @@ def ramp(scale: int = 1, seed: int = 1234, iterations: int = 200) -> Case:
     cfg = default_config(viscous=0, gradient=GRAD_LSQ_NODE, reconstruction=RECON_MUSCL, limiter=LIM_VENKATAKRISHNAN,
                          venkat_k=0.5, precond=PC_SGS, sgs_ordering=SGS_COLOR, precision=PREC_FP64,
                          lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
-                         cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8,
+                         cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))
     bcs = [bc(0, BC_SUPERSONIC_INLET, p=p, t=T, velocity=(u, 0.0, 0.0)),
            bc(1, BC_SUPERSONIC_OUTLET), bc(2, BC_SUPERSONIC_OUTLET), bc(3, BC_SLIP_WALL), bc(4, BC_SYMMETRY)]
@@ -90,7 +90,7 @@ def plate(scale: int = 1, seed: int = 4321, iterations: int = 200, mixed: bool =
                          venkat_k=0.5, precond=PC_SGS, sgs_ordering=SGS_COLOR,
                          precision=PREC_FP64 if not mixed else 1, prandtl=0.72,
                          lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
-                         cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8,
+                         cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))
     bcs = [bc(0, BC_SUBSONIC_INLET, p=p, t=T, velocity=(u, 0.0, 0.0)),
            bc(1, BC_SUBSONIC_OUTLET, p=p),
@@ -112,7 +112,7 @@ def bump(scale: int = 1, seed: int = 777, iterations: int = 200, mixed: bool = T
                          venkat_k=0.5, precond=PC_SGS, sgs_ordering=SGS_COLOR,
                          precision=1 if mixed else PREC_FP64,
                          lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
-                         cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8,
+                         cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))
     far = dict(p=p, t=T, velocity=(u, 0.0, 0.0))
     bcs = [bc(0, BC_FARFIELD, **far), bc(1, BC_FARFIELD, **far), bc(2, BC_FARFIELD, **far), bc(3, BC_SLIP_WALL),

@@ -233,16 +233,39 @@ __global__ void __launch_bounds__(256) k_krylov_init(int64_t len, const double* 
     block_reduce_store<2, 256>(pr, partials + size_t(blockIdx.x) * 2);
 }
 
-__device__ __forceinline__ double sum_partials(const double* __restrict__ partials, int nblocks, int stride, int k) {
+// Sum of column k of the per-block partials (stride values per block) by the
+// whole block: thread t adds blocks t, t+T, ... in order, then a fixed-order
+// tree; every thread returns the same total.  Deterministic for a given
+// partial count.
+constexpr int kFinThreads = 512;
+
+__device__ __forceinline__ double block_sum_partials(const double* __restrict__ partials, int nblocks, int stride,
+                                                     int k) {
+    __shared__ double sh[kFinThreads / 32];
+    __shared__ double total;
     double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[size_t(b) * stride + k];
-    return s;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[size_t(b) * stride + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sh[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+        double x = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) total = x;
+    }
+    __syncthreads();
+    const double r = total;
+    __syncthreads();
+    return r;
 }
 
 __global__ void k_krylov_init_fin(KrylovScalars* ks, const double* __restrict__ partials, int nblocks) {
+    const double bnorm = sqrt(block_sum_partials(partials, nblocks, 2, 0));
+    const double rnorm = sqrt(block_sum_partials(partials, nblocks, 2, 1));
     if (threadIdx.x != 0) return;
-    const double bnorm = sqrt(sum_partials(partials, nblocks, 2, 0));
-    const double rnorm = sqrt(sum_partials(partials, nblocks, 2, 1));
     const double scale = (bnorm > 0.0) ? bnorm : 1.0;
     ks->bnorm = bnorm;
     ks->scale = scale;
@@ -266,8 +289,9 @@ __global__ void k_krylov_init_fin(KrylovScalars* ks, const double* __restrict__ 
 // gamma = r0.v -> alpha = rho / gamma (bicgstab.cpp:112-119); also counts
 // the iteration and stops at max_it.
 __global__ void k_krylov_gamma(KrylovScalars* ks, const double* __restrict__ partials, int nblocks) {
-    if (threadIdx.x != 0 || ks->state != KS_RUNNING) return;
-    const double gamma = sum_partials(partials, nblocks, 1, 0);
+    if (ks->state != KS_RUNNING) return;  // uniform
+    const double gamma = block_sum_partials(partials, nblocks, 1, 0);
+    if (threadIdx.x != 0) return;
     if (!isfinite(gamma) || gamma == 0.0) {
         ks->state = KS_DIVERGED;
         return;
@@ -299,12 +323,13 @@ __global__ void __launch_bounds__(256) k_krylov_s(int64_t len, const KrylovScala
 // Five fused inner products -> omega, reconstructed |r|, rho_next
 // (bicgstab.cpp:128-158), pre-update breakdown checks.
 __global__ void k_krylov_omega(KrylovScalars* ks, const double* __restrict__ partials, int nblocks) {
-    if (threadIdx.x != 0 || ks->state != KS_RUNNING) return;
-    const double tt = sum_partials(partials, nblocks, 5, 0);
-    const double ts = sum_partials(partials, nblocks, 5, 1);
-    const double r0t = sum_partials(partials, nblocks, 5, 2);
-    const double r0s = sum_partials(partials, nblocks, 5, 3);
-    const double ss = sum_partials(partials, nblocks, 5, 4);
+    if (ks->state != KS_RUNNING) return;  // uniform
+    const double tt = block_sum_partials(partials, nblocks, 5, 0);
+    const double ts = block_sum_partials(partials, nblocks, 5, 1);
+    const double r0t = block_sum_partials(partials, nblocks, 5, 2);
+    const double r0s = block_sum_partials(partials, nblocks, 5, 3);
+    const double ss = block_sum_partials(partials, nblocks, 5, 4);
+    if (threadIdx.x != 0) return;
     if (!isfinite(ts) || !isfinite(tt) || tt == 0.0) {
         ks->state = KS_DIVERGED;
         return;
@@ -348,15 +373,18 @@ __global__ void __launch_bounds__(256) k_krylov_update(int64_t len, const Krylov
 // Post-update checks, refresh every 32 iterations, convergence test
 // (bicgstab.cpp:149-176).
 __global__ void k_krylov_post(KrylovScalars* ks, const double* __restrict__ partials, int nblocks) {
-    if (threadIdx.x != 0 || ks->state != KS_RUNNING) return;
+    if (ks->state != KS_RUNNING) return;  // uniform
+    const bool refresh = (ks->it % 32 == 0);
+    const double rr = refresh ? block_sum_partials(partials, nblocks, 1, 0) : 0.0;
+    if (threadIdx.x != 0) return;
     const double omega_new = ks->omega_new;
     double rnorm = ks->rnorm;
     if (!isfinite(rnorm) || !isfinite(omega_new) || omega_new == 0.0) {
         ks->state = KS_DIVERGED;
         return;
     }
-    if (ks->it % 32 == 0) {
-        rnorm = sqrt(sum_partials(partials, nblocks, 1, 0));
+    if (refresh) {
+        rnorm = sqrt(rr);
         ks->rnorm = rnorm;
     }
     if (rnorm <= ks->tol) {
@@ -461,18 +489,18 @@ void launch_krylov_init(int64_t len, const double* b, const double* v, double* r
                         double* partials, KrylovScalars* ks, cudaStream_t s) {
     const unsigned gr = grid_for(len, 256);
     k_krylov_init<<<gr, 256, 0, s>>>(len, b, v, r, r0, p, partials);
-    k_krylov_init_fin<<<1, 32, 0, s>>>(ks, partials, static_cast<int>(gr));
+    k_krylov_init_fin<<<1, kFinThreads, 0, s>>>(ks, partials, static_cast<int>(gr));
 }
 void launch_krylov_begin(KrylovScalars* ks, cudaStream_t s) { k_krylov_begin<<<1, 32, 0, s>>>(ks); }
 void launch_krylov_gamma(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s) {
-    k_krylov_gamma<<<1, 32, 0, s>>>(ks, partials, nblocks);
+    k_krylov_gamma<<<1, kFinThreads, 0, s>>>(ks, partials, nblocks);
 }
 void launch_krylov_s(int64_t len, const KrylovScalars* ks, const double* r, const double* v, double* sv,
                      cudaStream_t s) {
     k_krylov_s<<<grid_for(len, 256), 256, 0, s>>>(len, ks, r, v, sv);
 }
 void launch_krylov_omega(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s) {
-    k_krylov_omega<<<1, 32, 0, s>>>(ks, partials, nblocks);
+    k_krylov_omega<<<1, kFinThreads, 0, s>>>(ks, partials, nblocks);
 }
 void launch_krylov_update(int64_t len, const KrylovScalars* ks, double* x, const double* phat, const double* shat,
                           const double* sv, const double* tv, double* r, double* p, const double* v,
@@ -480,7 +508,7 @@ void launch_krylov_update(int64_t len, const KrylovScalars* ks, double* x, const
     k_krylov_update<<<grid_for(len, 256), 256, 0, s>>>(len, ks, x, phat, shat, sv, tv, r, p, v, partials);
 }
 void launch_krylov_post(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s) {
-    k_krylov_post<<<1, 32, 0, s>>>(ks, partials, nblocks);
+    k_krylov_post<<<1, kFinThreads, 0, s>>>(ks, partials, nblocks);
 }
 
 template void launch_spmv_ex<double>(const BsrView&, const double*, const double*, double*, double, double,

@@ -250,13 +250,17 @@ __global__ void __launch_bounds__(256) k_norm_partials(int32_t n, const double* 
     block_reduce_store<NV, 256>(sq, partials + size_t(blockIdx.x) * NV);
 }
 
+// Warp v sums column v of the partials (lane-strided, then a fixed shuffle
+// tree): deterministic for a given block count.
 __global__ void k_norm_finalize(int nblocks, int nv, const double* __restrict__ partials, double scale,
                                 double* __restrict__ l2) {
-    const int v = threadIdx.x;
+    const int v = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (v >= nv) return;
     double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[size_t(b) * nv + v];
-    l2[v] = sqrt(s * scale);
+    for (int b = lane; b < nblocks; b += 32) s += partials[size_t(b) * nv + v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) l2[v] = sqrt(s * scale);
 }
 
 // compute_dt (solver.hpp:263-277) fused with set_rhs_and_zero_du
@@ -350,7 +354,7 @@ void launch_norms(int32_t n, int nv, const double* res, double* partials, double
     const unsigned gr = grid_for(n, 256);
     if (nv == 6) k_norm_partials<6><<<gr, 256, 0, s>>>(n, res, partials);
     else k_norm_partials<5><<<gr, 256, 0, s>>>(n, res, partials);
-    k_norm_finalize<<<1, 32, 0, s>>>(static_cast<int>(gr), nv, partials, 1.0 / double(n > 0 ? n : 1), l2);
+    k_norm_finalize<<<1, 32 * 6, 0, s>>>(static_cast<int>(gr), nv, partials, 1.0 / double(n > 0 ? n : 1), l2);
 }
 
 void launch_dt_rhs(const DevMesh& m, const DevFields& f, int nv, double cfl, double* b, double* du, cudaStream_t s) {

@@ -1022,36 +1022,54 @@ double Solver::cfl_at(int64_t iter) const {
     return std::min(cfg_.cfl_max, cfg_.cfl * std::pow(cfg_.cfl_max / cfg_.cfl, t));
 }
 
-// Solver::run_steady (solver.hpp:597-660).
+// Solver::run_steady (solver.hpp:597-660) with the CFL ramp and the
+// selected convergence monitor.
 cfdg_run_result Solver::run_steady() {
     cfdg_run_result out{};
     const auto t0 = std::chrono::steady_clock::now();
-    double norm0[6] = {0, 0, 0, 0, 0, 0};
+    double ref_norm[6] = {0, 0, 0, 0, 0, 0};
     bool have0 = false;
     const int interval = std::max(cfg_.residual_interval, 1);
+    const bool robust = cfg_.convergence_monitor == 1;
     for (int64_t iter = 1; iter <= cfg_.max_iterations; ++iter) {
         const cfdg_step_result st = newton_step(cfl_at(iter));
         out.iterations = iter;
         out.krylov_iterations_total += st.krylov_iterations;
         const bool diagnose = iter == 1 || iter % interval == 0 || iter == cfg_.max_iterations;
         if (!diagnose) continue;
-        if (!std::isfinite(st.l2[0])) {
+        bool finite = true;
+        for (int v = 0; v < nv_; ++v) finite = finite && std::isfinite(st.l2[v]);
+        if (!finite) {
             out.blowup = 1;
             break;
         }
         for (int v = 0; v < nv_; ++v) out.l2_last[v] = st.l2[v];
+        // monitored components
+        double mon[6];
+        int nm = 0;
+        if (robust) {
+            mon[nm++] = st.l2[0];
+            mon[nm++] = std::sqrt(st.l2[1] * st.l2[1] + st.l2[2] * st.l2[2] + st.l2[3] * st.l2[3]);
+            mon[nm++] = st.l2[4];
+            if (nv_ == 6) mon[nm++] = st.l2[5];
+        } else {
+            for (int v = 0; v < nv_; ++v) mon[nm++] = st.l2[v];
+        }
         if (!have0) {
-            for (int v = 0; v < nv_; ++v) norm0[v] = out.l2_first[v] = st.l2[v];
+            for (int v = 0; v < nv_; ++v) out.l2_first[v] = st.l2[v];
+            for (int k = 0; k < nm; ++k) ref_norm[k] = mon[k];
             have0 = true;
             out.rel = 1.0;
-        } else {
-            double rel = 0.0;
-            for (int v = 0; v < nv_; ++v) rel = std::max(rel, st.l2[v] / std::max(norm0[v], 1.0e-300));
-            out.rel = rel;
-            if (rel <= cfg_.residual_tolerance) {
-                out.converged = 1;
-                break;
-            }
+            continue;
+        }
+        if (robust)
+            for (int k = 0; k < nm; ++k) ref_norm[k] = std::max(ref_norm[k], mon[k]);
+        double rel = 0.0;
+        for (int k = 0; k < nm; ++k) rel = std::max(rel, mon[k] / std::max(ref_norm[k], 1.0e-300));
+        out.rel = rel;
+        if (rel <= cfg_.residual_tolerance) {
+            out.converged = 1;
+            break;
         }
     }
     out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -161,6 +161,13 @@ typedef struct cfdg_config {
     int32_t lin_max_iterations;
     int32_t cfl_ramp_iterations; /* iterations over which CFL goes cfl->cfl_max */
     int32_t residual_interval;
+    /* 0: the reference monitor, max over variables of L2_v / L2_v(first
+     *    diagnosed iteration) (solver.hpp:631-636,758-765);
+     * 1: max over (mass, |momentum|, energy[, nu_tilde]) of L2 / running
+     *    maximum of L2 (robust when a component starts at round-off, e.g.
+     *    spanwise momentum of a quasi-2-D case or a uniform initial state). */
+    int32_t convergence_monitor;
+    int32_t reserved_;
     double gamma, gas_constant, prandtl, prandtl_turb;
     double init_rho, init_p, init_velocity[3];
     double venkat_k;
