@@ -109,16 +109,24 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def _case(cb, name: str, precision: str):
+def _case(cb, name: str, precision: str, scale: int = 1):
     mixed = precision == "mixed"
     if name == "plate":
-        case = cb.cases.plate(mixed=mixed)
+        case = cb.cases.plate(scale=scale, mixed=mixed)
     elif name == "ramp":
-        case = cb.cases.ramp()
+        case = cb.cases.ramp(scale=scale)
         case.cfg.precision = 1 if mixed else 0
     else:
-        case = cb.cases.bump(mixed=mixed)
+        case = cb.cases.bump(scale=scale, mixed=mixed)
+    if scale != 1:
+        case.description += f" (cell counts divided by {scale}^3)"
     return case
+
+
+# DRAM bytes (read + write) per algorithmic byte of a kernel family, from an
+# ncu capture of the same kernel on the 1/8-size plate, scaled to a full
+# launch by the rows it processes (profiles/sgs_rows_plate_scale2.md).
+TRAFFIC_PER_ALG_BYTE = {"sgs": 108.9 / 100.2}
 
 
 def _roofline(prof: dict, peak: float, peak_kind: str):
@@ -134,7 +142,8 @@ def _roofline(prof: dict, peak: float, peak_kind: str):
              for k, v in sorted(fams.items(), key=lambda kv: -kv[1]["ms"])}
     return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-            "bytes_per_launch": per_launch_bytes, "avg_launch_ms": per_launch_ms, "traffic": None,
+            "bytes_per_launch": per_launch_bytes, "avg_launch_ms": per_launch_ms,
+            "traffic": (round(per_launch_bytes * TRAFFIC_PER_ALG_BYTE[dom]) if dom in TRAFFIC_PER_ALG_BYTE else None),
             "families": table}
 
 
@@ -168,7 +177,7 @@ def run_reference(args):
     import __graft_entry__ as ge
     cb = ge.load_package()
     refh, port = ge.load_oracle()
-    case = _case(cb, args.case, "fp64")
+    case = _case(cb, args.case, "fp64", args.scale)
     mesh = cb.HostMesh(case.spec)
     if not refh.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcfdref.so was not built"}))
@@ -205,7 +214,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         pg = dist
-    case = _case(cb, args.case, args.precision)
+    case = _case(cb, args.case, args.precision, args.scale)
     mesh = cb.HostMesh(case.spec)
     n = mesh.n_cells
     s = cb.Solver(mesh, case.cfg, case.bcs, device=local)
@@ -323,6 +332,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default="plate", choices=["plate", "ramp", "bump"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--scale", type=int, default=1, help="divide each mesh dimension (profiling runs)")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

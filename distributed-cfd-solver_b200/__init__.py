@@ -339,7 +339,11 @@ class Solver:
                 FIELD_WALLDIST: n, FIELD_RHS: n * self.nvars}[field]
 
     def get(self, field: int) -> np.ndarray:
-        out = np.empty(self.field_size(field), dtype=np.float64)
+        try:
+            size = self.field_size(field)
+        except KeyError:
+            size = 1  # unknown field id: let the library report it
+        out = np.empty(size, dtype=np.float64)
         check(lib().cfdg_solver_get_field(self._h, field, _dptr(out), out.size))
         return out
 

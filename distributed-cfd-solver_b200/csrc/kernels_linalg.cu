@@ -117,7 +117,13 @@ __global__ void k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu
     for (int e = 0; e < BS * BS; ++e) dst[e] = static_cast<MT>(a[e]);
 #pragma unroll
     for (int k = 0; k < BS; ++k) piv[int64_t(i) * BS + k] = pv[k];
-    if (!ok || !isfinite(a[BS * BS - 1])) {
+    // +(i+1): zero pivot (singular block); -(i+1): non-finite entries
+    bool finite = true;
+#pragma unroll
+    for (int e = 0; e < BS * BS; ++e) finite = finite && isfinite(a[e]);
+    if (!finite) {
+        atomicCAS(err, 0, -(i + 1));
+    } else if (!ok) {
         atomicCAS(err, 0, i + 1);
     }
 }

@@ -381,8 +381,11 @@ void BsrSystem::sgs_setup(int ordering, int sweeps) {
     int err = 0;
     cuda_check(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
     cuda_check(cudaStreamSynchronize(stream_), "lu sync");
-    if (err != 0) {
+    if (err > 0) {
         throw Failure{CFDG_ERR_SINGULAR, "SgsPreconditioner: singular diagonal block at row " + std::to_string(err - 1)};
+    }
+    if (err < 0) {
+        throw Failure{CFDG_ERR_NONFINITE, "SgsPreconditioner: non-finite diagonal block at row " + std::to_string(-err - 1)};
     }
     lu_ready_ = true;
 }
@@ -1032,7 +1035,17 @@ cfdg_run_result Solver::run_steady() {
     const int interval = std::max(cfg_.residual_interval, 1);
     const bool robust = cfg_.convergence_monitor == 1;
     for (int64_t iter = 1; iter <= cfg_.max_iterations; ++iter) {
-        const cfdg_step_result st = newton_step(cfl_at(iter));
+        cfdg_step_result st;
+        try {
+            st = newton_step(cfl_at(iter));
+        } catch (const Failure& f) {
+            // a non-finite state shows up in the diagonal blocks before the
+            // residual norms: the reference's "blowup" exit (solver.hpp:625-629)
+            if (f.status != CFDG_ERR_NONFINITE) throw;
+            out.iterations = iter;
+            out.blowup = 1;
+            break;
+        }
         out.iterations = iter;
         out.krylov_iterations_total += st.krylov_iterations;
         const bool diagnose = iter == 1 || iter % interval == 0 || iter == cfg_.max_iterations;
