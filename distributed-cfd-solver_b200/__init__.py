@@ -146,6 +146,7 @@ _SIGS = {
     "cfdg_newton_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(StepResult)]),
     "cfdg_residual_norms": (C.c_int, [C.c_void_p, _dp]),
     "cfdg_run_steady": (C.c_int, [C.c_void_p, C.POINTER(RunResult)]),
+    "cfdg_residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, _dp]),
     "cfdg_solver_stream": (C.c_void_p, [C.c_void_p]),
     "cfdg_solver_launch_count": (C.c_int64, [C.c_void_p]),
     "cfdg_solver_profile": (C.c_int, [C.c_void_p, C.c_int32]),

@@ -265,6 +265,19 @@ CFDG_API int cfdg_linear_solve(cfdg_solver* s, cfdg_krylov_result* out_h);
 CFDG_API int cfdg_newton_step(cfdg_solver* s, double cfl, cfdg_step_result* out_h);
 /* Solver::residual_norms (solver.hpp:740-756), nvars doubles. */
 CFDG_API int cfdg_residual_norms(cfdg_solver* s, double* l2_h);
+/* Allocation-free variant of cfdg_residual_norms, with no counterpart in the
+ * reference: per-variable L2 norms sqrt(sum_c r_v[c]^2 / n_cells) of an SoA
+ * device array (nvars x n_cells doubles) the caller owns, for callers that
+ * cannot allocate device memory (a host code whose pool owns the whole device
+ * budget, or a hook between solver kernels where cudaMalloc would
+ * synchronise).  Scratch is a static 768 KiB device array: nvars <= 6 and
+ * n_cells <= 4,194,304, larger sizes return CFDG_ERR_INVALID.  stream may be
+ * NULL (legacy default stream); the call synchronises it.  Calls share the
+ * scratch, so calls that overlap on the GPU race; the first call on a device
+ * looks up the scratch address there and should come before any stream
+ * capture. */
+CFDG_API int cfdg_residual_norms_noalloc(const double* res_d, int32_t n_cells, int32_t nvars, void* stream,
+                                         double* l2_h);
 /* Solver::run_steady (solver.hpp:597-660) with the CFL ramp. */
 CFDG_API int cfdg_run_steady(cfdg_solver* s, cfdg_run_result* out_h);
 /* Stream all solver kernels are queued on (cudaStream_t as void*). */
