@@ -30,13 +30,34 @@ __device__ __forceinline__ void side_jacobian(const GasParams& g, const double U
     for (int i = 0; i < 5; ++i) J[i * 6] += diss;
 }
 
+// Stores the block each lane of the warp holds in `stage[lane]` to its BSR
+// slot: the warp walks its 32 faces and writes one contiguous block per step
+// (coalesced), instead of 32 scattered 8-byte stores per instruction.
+template <typename MT, int BS>
+__device__ __forceinline__ void warp_store_blocks(MT (*stage)[BS * BS], int32_t pos, bool valid, MT* vals) {
+    __syncwarp();
+    const int lane = threadIdx.x & 31;
+    for (int src = 0; src < 32; ++src) {
+        const int32_t p = __shfl_sync(0xffffffffu, pos, src);
+        const int ok = __shfl_sync(0xffffffffu, valid ? 1 : 0, src);
+        if (!ok) continue;
+        MT* dst = vals + int64_t(p) * (BS * BS);
+        for (int e = lane; e < BS * BS; e += 32) dst[e] = stage[src][e];
+    }
+    __syncwarp();
+}
+
 template <typename MT, bool VISC, int BS>
 __global__ void __launch_bounds__(128) k_jac_offdiag(DevMesh m, DevFields f, GasParams g, JacStructure js, MT* vals) {
+    __shared__ MT stage_all[4][32][BS * BS];
+    MT(*stage)[BS * BS] = stage_all[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
     const int32_t fc = blockIdx.x * blockDim.x + threadIdx.x;
-    if (fc >= m.ni) return;
+    const bool valid = fc < m.ni;
+    const int32_t fcs = valid ? fc : 0;  // lanes past the end compute on face 0 and store nothing
     const int64_t nt = m.nt;
-    const int32_t c0 = m.owner[fc], c1 = m.neigh[fc];
-    const double nx = m.fnx[fc], ny = m.fny[fc], nz = m.fnz[fc], A = m.farea[fc];
+    const int32_t c0 = m.owner[fcs], c1 = m.neigh[fcs];
+    const double nx = m.fnx[fcs], ny = m.fny[fcs], nz = m.fnz[fcs], A = m.farea[fcs];
     double qL[5], qR[5], UL[5], UR[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -55,34 +76,20 @@ __global__ void __launch_bounds__(128) k_jac_offdiag(DevMesh m, DevFields f, Gas
     double J[25];
     // A(c0, c1) += dF/dUR
     side_jacobian(g, UR, nx, ny, nz, half_area, -diss, J);
-    if (VISC) viscous_jacobian_add(g, m.finv_d[fc], qL, qR, mutL, mutR, A, -1.0, J);
-    {
-        MT* dst = vals + int64_t(js.face_pos[2 * fc]) * (BS * BS);
-        if (BS == 5) {
+    if (VISC) viscous_jacobian_add(g, m.finv_d[fcs], qL, qR, mutL, mutR, A, -1.0, J);
 #pragma unroll
-            for (int i = 0; i < 25; ++i) dst[i] = to_mt<MT>(J[i]);
-        } else {
+    for (int r = 0; r < BS; ++r)
 #pragma unroll
-            for (int r = 0; r < BS; ++r)
-#pragma unroll
-                for (int c = 0; c < BS; ++c) dst[r * BS + c] = (r < 5 && c < 5) ? to_mt<MT>(J[r * 5 + c]) : MT(0);
-        }
-    }
+        for (int c = 0; c < BS; ++c) stage[lane][r * BS + c] = (r < 5 && c < 5) ? to_mt<MT>(J[r * 5 + c]) : MT(0);
+    warp_store_blocks<MT, BS>(stage, js.face_pos[2 * fcs], valid, vals);
     // A(c1, c0) -= dF/dUL
     side_jacobian(g, UL, nx, ny, nz, half_area, diss, J);
-    if (VISC) viscous_jacobian_add(g, m.finv_d[fc], qL, qR, mutL, mutR, A, 1.0, J);
-    {
-        MT* dst = vals + int64_t(js.face_pos[2 * fc + 1]) * (BS * BS);
-        if (BS == 5) {
+    if (VISC) viscous_jacobian_add(g, m.finv_d[fcs], qL, qR, mutL, mutR, A, 1.0, J);
 #pragma unroll
-            for (int i = 0; i < 25; ++i) dst[i] = to_mt<MT>(-J[i]);
-        } else {
+    for (int r = 0; r < BS; ++r)
 #pragma unroll
-            for (int r = 0; r < BS; ++r)
-#pragma unroll
-                for (int c = 0; c < BS; ++c) dst[r * BS + c] = (r < 5 && c < 5) ? to_mt<MT>(-J[r * 5 + c]) : MT(0);
-        }
-    }
+        for (int c = 0; c < BS; ++c) stage[lane][r * BS + c] = (r < 5 && c < 5) ? to_mt<MT>(-J[r * 5 + c]) : MT(0);
+    warp_store_blocks<MT, BS>(stage, js.face_pos[2 * fcs + 1], valid, vals);
 }
 
 // Boundary faces: owner-side block only, first-order states against the BC

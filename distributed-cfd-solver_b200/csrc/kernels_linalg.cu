@@ -121,10 +121,10 @@ __global__ void k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu
     bool finite = true;
 #pragma unroll
     for (int e = 0; e < BS * BS; ++e) finite = finite && isfinite(a[e]);
-    if (!finite) {
-        atomicCAS(err, 0, -(i + 1));
-    } else if (!ok) {
+    if (!ok) {
         atomicCAS(err, 0, i + 1);
+    } else if (!finite) {
+        atomicCAS(err, 0, -(i + 1));
     }
 }
 
