@@ -116,6 +116,8 @@ def _case(cb, name: str, precision: str, scale: int = 1):
     elif name == "ramp":
         case = cb.cases.ramp(scale=scale)
         case.cfg.precision = 1 if mixed else 0
+    elif name == "sa_plate":
+        case = cb.cases.sa_plate(scale=scale, mixed=mixed)
     else:
         case = cb.cases.bump(scale=scale, mixed=mixed)
     if scale != 1:
@@ -316,12 +318,8 @@ def run_ours(args):
 
 
 def _cfl(case, it):
-    cfg = case.cfg
-    K = cfg.cfl_ramp_iterations
-    if K <= 1 or cfg.cfl_max <= cfg.cfl:
-        return cfg.cfl
-    t = min(1.0, (it - 1) / (K - 1))
-    return min(cfg.cfl_max, cfg.cfl * (cfg.cfl_max / cfg.cfl) ** t)
+    import __graft_entry__ as ge
+    return ge.load_package().cases.cfl_at(case.cfg, it)
 
 
 def main():
@@ -330,7 +328,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--case", default="plate", choices=["plate", "ramp", "bump"])
+    ap.add_argument("--case", default="plate", choices=["plate", "ramp", "bump", "sa_plate"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--scale", type=int, default=1, help="divide each mesh dimension (profiling runs)")
     ap.add_argument("--cpu-steps", type=int, default=2)

@@ -43,10 +43,10 @@ PREC_FP64, PREC_MIXED = 0, 1
 PC_NONE, PC_SGS = 0, 1
 KRYLOV_CONVERGED, KRYLOV_DIVERGED, KRYLOV_MAX_ITERATIONS = 0, 1, 2
 (FIELD_U, FIELD_Q, FIELD_GRAD, FIELD_PHI, FIELD_RES, FIELD_LAM, FIELD_DT, FIELD_ALPHA, FIELD_JAC, FIELD_DU,
- FIELD_MUT, FIELD_WALLDIST, FIELD_RHS) = range(13)
+ FIELD_MUT, FIELD_WALLDIST, FIELD_RHS, FIELD_NU, FIELD_NU_GRAD) = range(15)
 STAGE_PRIMITIVES, STAGE_GRADIENT, STAGE_LIMITER, STAGE_FLUXES = range(4)
 KCAT_NAMES = ("primitives", "gradient", "limiter", "face_flux", "cell_gather", "jacobian", "lu", "spmv", "sgs",
-              "krylov", "update")
+              "krylov", "update", "turbulence")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -337,7 +337,7 @@ class Solver:
         return {FIELD_U: n * self.nvars, FIELD_Q: nt * 5, FIELD_GRAD: nt * 3 * self.nvars, FIELD_PHI: n * 5,
                 FIELD_RES: n * self.nvars, FIELD_LAM: n, FIELD_DT: n, FIELD_ALPHA: n,
                 FIELD_JAC: self.nnzb * self.bs * self.bs, FIELD_DU: n * self.nvars, FIELD_MUT: nt,
-                FIELD_WALLDIST: n, FIELD_RHS: n * self.nvars}[field]
+                FIELD_WALLDIST: n, FIELD_RHS: n * self.nvars, FIELD_NU: n, FIELD_NU_GRAD: 3 * nt}[field]
 
     def get(self, field: int) -> np.ndarray:
         try:

@@ -7,6 +7,8 @@ synthetic inputs (the reference ships no meshes or datasets):
   plate - laminar Navier-Stokes flat plate, M=0.5, Re_L=1e5, 256x128x32 hex,
           wall-normal stretching 1.08 from 1e-5 L, +-10% node jitter
   bump  - transonic Euler bump (M=0.85) on 160x80x80 hex split into 6 tets
+  sa_plate - Spalart-Allmaras RANS flat plate, M=0.2, Re_L=5e6, 384x192x56
+          hex, wall-normal stretching 1.1 from 1e-6 L, +-5% node jitter
 
 Every case takes a `scale` that divides the cell counts for the parity tests.
 Free-stream states follow from (M, T, p) or (M, Re_L, T) with the ideal gas
@@ -101,6 +103,33 @@ def plate(scale: int = 1, seed: int = 4321, iterations: int = 200, mixed: bool =
                 {"mach": M, "Re": Re, "T": T, "p": p, "rho": rho, "u": u})
 
 
+def sa_plate(scale: int = 1, seed: int = 2468, iterations: int = 200, mixed: bool = True) -> Case:
+    """Spalart-Allmaras RANS flat plate, M=0.2, Re_L=5e6, free-stream
+    nu_tilde/nu = 3 (384x192x56 hex, 4,128,768 cells); wall-normal growth 1.1
+    from 1e-6 L, capped at 0.01 L."""
+    nx, ny, nz = max(384 // scale, 8), max(192 // scale, 8), max(56 // scale, 2)
+    T, M, Re, L = 288.15, 0.2, 5.0e6, 1.0
+    u = M * sound_speed(T)
+    mu = sutherland(T)
+    rho = Re * mu / (u * L)
+    p = rho * R_GAS * T
+    spec = _spec(1, nx, ny, nz, 1.25 * L, 0.0, 0.1 * L, seed, first_spacing=1.0e-6 * L * scale,
+                 stretch=1.1 ** scale, cap_spacing=0.01 * L * scale, jitter=0.05, plate_x0=0.25 * L)
+    cfg = default_config(viscous=1, turbulence=1, nu_inf_ratio=3.0, gradient=GRAD_LSQ_NODE,
+                         reconstruction=RECON_MUSCL, limiter=LIM_VENKATAKRISHNAN, venkat_k=0.5, precond=PC_SGS,
+                         sgs_ordering=SGS_COLOR, precision=1 if mixed else PREC_FP64, prandtl=0.72,
+                         lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
+                         cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
+                         init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))
+    bcs = [bc(0, BC_SUBSONIC_INLET, p=p, t=T, velocity=(u, 0.0, 0.0)),
+           bc(1, BC_SUBSONIC_OUTLET, p=p),
+           bc(2, BC_FARFIELD, p=p, t=T, velocity=(u, 0.0, 0.0)),
+           bc(3, BC_NO_SLIP_WALL_HEAT_FLUX, tmp_grad=0.0),
+           bc(4, BC_SYMMETRY), bc(5, BC_SYMMETRY)]
+    return Case("sa_plate", spec, cfg, bcs, iterations, "SA RANS flat plate M=0.2 Re_L=5e6, 384x192x56 hex",
+                {"mach": M, "Re": Re, "T": T, "p": p, "rho": rho, "u": u, "nu_inf": 3.0 * mu / rho})
+
+
 def bump(scale: int = 1, seed: int = 777, iterations: int = 200, mixed: bool = True) -> Case:
     """Transonic Euler bump, M=0.85, 160x80x80 hex -> 6 tets each (6,144,000 cells)."""
     nx, ny, nz = max(160 // scale, 6), max(80 // scale, 3), max(80 // scale, 3)
@@ -121,17 +150,32 @@ def bump(scale: int = 1, seed: int = 777, iterations: int = 200, mixed: bool = T
                 {"mach": M, "T": T, "p": p})
 
 
+def cfl_at(cfg, it: int) -> float:
+    """CFL of nonlinear iteration `it` (1-based): geometric ramp from cfg.cfl
+    to cfg.cfl_max over cfg.cfl_ramp_iterations (the library's run_steady
+    schedule)."""
+    K = cfg.cfl_ramp_iterations
+    if K <= 1 or not cfg.cfl_max > cfg.cfl:
+        return cfg.cfl
+    t = min(1.0, (it - 1) / (K - 1))
+    return min(cfg.cfl_max, cfg.cfl * (cfg.cfl_max / cfg.cfl) ** t)
+
+
 def freestream_state(case: Case, n: int):
-    """Conserved state U (5 x n) of the case's uniform initial condition."""
+    """Conserved state U (5 x n, 6 x n with Spalart-Allmaras) of the case's
+    uniform initial condition."""
     import numpy as np
     cfg = case.cfg
     rho, p = cfg.init_rho, cfg.init_p
     u, v, w = cfg.init_velocity[0], cfg.init_velocity[1], cfg.init_velocity[2]
     T = p / (rho * R_GAS)
     e = R_GAS / (GAMMA - 1.0) * T
-    U = np.empty((5, n))
+    sa = bool(cfg.turbulence)
+    U = np.empty((6 if sa else 5, n))
     U[0], U[1], U[2], U[3] = rho, rho * u, rho * v, rho * w
     U[4] = rho * e + 0.5 * rho * (u * u + v * v + w * w)
+    if sa:
+        U[5] = cfg.nu_inf_ratio * sutherland(T) / rho * rho
     return U
 
 
@@ -142,7 +186,7 @@ def perturbed_state(case: Case, n: int, seed: int = 5, amplitude: float = 0.02):
     rng = np.random.default_rng(seed)
     U = freestream_state(case, n)
     base = U.copy()
-    for k in range(5):
+    for k in range(U.shape[0]):
         U[k] = base[k] * (1.0 + amplitude * rng.uniform(-1.0, 1.0, size=n))
     # keep the velocity perturbation relative to the free-stream speed
     spd = max(abs(case.cfg.init_velocity[0]), 1.0) * base[0]

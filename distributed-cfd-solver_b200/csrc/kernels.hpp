@@ -54,11 +54,11 @@ struct SaParams {
     double nu_inf;      // freestream specific nu_tilde
     double sigma, cb1, cb2, kappa, cw1, cw2, cw3, cv1;
 };
-void launch_sa_pre(const DevMesh& m, const DevFields& f, const GasParams& g, const SaParams& sa, cudaStream_t s);
-void launch_sa_face_sweep(const DevMesh& m, const DevFields& f, const GasParams& g, const SaParams& sa,
-                          double* sa_face, cudaStream_t s);
-void launch_sa_cell(const DevMesh& m, const DevFields& f, const GasParams& g, const SaParams& sa,
-                    const double* sa_face, cudaStream_t s);
+void launch_sa_pre(const DevMesh& m, const DevFields& f, const GasParams& g, const SaParams& sa, double* rhonu_g,
+                   cudaStream_t s);
+void launch_sa_sweep(const DevMesh& m, const DevFields& f, const GasParams& g, const SaParams& sa,
+                     const double* rhonu_g, const double* gnu, double* face, double* jac, double* dsrc,
+                     cudaStream_t s);
 
 // ---------------------------------------------------------------- Jacobian
 struct JacStructure {
@@ -71,6 +71,9 @@ struct JacStructure {
 template <typename MT>
 void launch_jacobian(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,
                      bool visc, MT* values, double* bface_scratch, cudaStream_t s);
+template <typename MT>
+void launch_sa_jacobian(const DevMesh& m, const DevFields& f, const JacStructure& js, const double* jac,
+                        const double* dsrc, MT* vals, cudaStream_t s);
 
 // ------------------------------------------------------------ linear algebra
 struct BsrView {

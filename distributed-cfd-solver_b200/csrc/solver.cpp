@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <queue>
 
 namespace cfdg {
 
@@ -843,8 +844,87 @@ void Solver::setup_matrix(const HostMesh& hm, const Csr& c2c) {
     cuda_check(cudaStreamSynchronize(stream_), "setup sync");
 }
 
-void Solver::setup_sa(const HostMesh&) {
-    throw Failure{CFDG_ERR_UNSUPPORTED, "Spalart-Allmaras module not built in this library"};
+// Graph distance to the no-slip walls over the face-neighbour stencil: each
+// wall face seeds its owner with the owner-to-face-centroid distance, edges
+// weigh the centroid distance.  Dijkstra returns the fixed point that the
+// reference's Gauss-Seidel relaxation converges to
+// (MeshAuxGeometry::add_wall_distance, src/mesh/aux_geometry.cpp:609-696,
+// relax_distance_graph :545-604); cells with no path keep 1e30 as there.
+static std::vector<double> graph_wall_distance(const HostMesh& hm, const Csr& c2c,
+                                               const std::vector<BcPatch>& patches) {
+    const int32_t n = hm.n_cells;
+    std::vector<double> d(static_cast<std::size_t>(n), 1.0e30);
+    for (int32_t f = hm.n_inner; f < hm.n_faces; ++f) {
+        if (patches[hm.patch[f]].sa_kind != 0) continue;
+        const int32_t c = hm.owner[f];
+        const double ex = hm.fcx[f] - hm.ccx[c], ey = hm.fcy[f] - hm.ccy[c], ez = hm.fcz[f] - hm.ccz[c];
+        d[c] = std::min(d[c], std::sqrt(ex * ex + ey * ey + ez * ez));
+    }
+    using Item = std::pair<double, int32_t>;
+    std::priority_queue<Item, std::vector<Item>, std::greater<Item>> heap;
+    for (int32_t c = 0; c < n; ++c)
+        if (d[c] < 1.0e30) heap.emplace(d[c], c);
+    std::vector<uint8_t> done(static_cast<std::size_t>(n), 0);
+    while (!heap.empty()) {
+        const auto [du, u] = heap.top();
+        heap.pop();
+        if (done[u] || du > d[u]) continue;
+        done[u] = 1;
+        for (int32_t k = c2c.off[u]; k < c2c.off[u + 1]; ++k) {
+            const int32_t v = c2c.val[k];
+            if (done[v]) continue;
+            const double dx = hm.ccx[u] - hm.ccx[v], dy = hm.ccy[u] - hm.ccy[v], dz = hm.ccz[u] - hm.ccz[v];
+            const double cand = du + std::sqrt(dx * dx + dy * dy + dz * dz);
+            if (cand < d[v]) {
+                d[v] = cand;
+                heap.emplace(cand, v);
+            }
+        }
+    }
+    return d;
+}
+
+// SpalartAllmaras::initialize (turbulence/spalart_allmaras.hpp:180-200):
+// model constants, freestream nu_tilde = ratio * mu(T_inf) / rho_inf, wall
+// distance, and the turbulence work arrays.
+void Solver::setup_sa(const HostMesh& hm) {
+    sap_.sigma = 2.0 / 3.0;
+    sap_.cb1 = 0.1355;
+    sap_.cb2 = 0.622;
+    sap_.kappa = 0.41;
+    sap_.cw2 = 0.3;
+    sap_.cw3 = 2.0;
+    sap_.cv1 = 7.1;
+    sap_.cw1 = sap_.cb1 / (sap_.kappa * sap_.kappa) + (1.0 + sap_.cb2) / sap_.sigma;
+    const double T_inf = cfg_.init_p / (cfg_.init_rho * gas_.R);
+    constexpr double mu_ref = 1.716e-5, T_ref = 273.15, S_suth = 110.4;
+    const double mu_inf = mu_ref * std::pow(T_inf / T_ref, 1.5) * (T_ref + S_suth) / (T_inf + S_suth);
+    sap_.nu_inf = cfg_.nu_inf_ratio * mu_inf / cfg_.init_rho;
+    const Csr c2c = build_cell_cells_face(hm);
+    const std::vector<double> wd = graph_wall_distance(hm, c2c, patches_h_);
+    upload_or_throw(wall_dist_, wd, stream_, "wall distance");
+    const std::size_t n = static_cast<std::size_t>(dm_.n), nt = static_cast<std::size_t>(dm_.nt);
+    const std::size_t nf = static_cast<std::size_t>(dm_.nf), nb = static_cast<std::size_t>(std::max(dm_.nb, 1));
+    alloc_or_throw(nu_, nt, "nu_tilde");
+    alloc_or_throw(rho_, nt, "rho");
+    alloc_or_throw(mut_, nt, "mu_t");
+    alloc_or_throw(rhonu_g_, nb, "ghost rho nu_tilde");
+    alloc_or_throw(sa_face_, 2 * nf, "SA face");
+    alloc_or_throw(sa_jac_, 2 * nf, "SA face jacobian");
+    alloc_or_throw(sa_dsrc_, n, "SA destruction derivative");
+    for (DevArray<double>* a : {&nu_, &rho_, &mut_, &rhonu_g_, &sa_face_, &sa_jac_, &sa_dsrc_})
+        cuda_check(cudaMemsetAsync(a->p, 0, a->count * sizeof(double), stream_), "memset");
+    cuda_check(cudaStreamSynchronize(stream_), "setup sync");
+    dm_.wall_dist = wall_dist_.p;
+    df_.nu = nu_.p;
+    df_.rho = rho_.p;
+    df_.mut = mut_.p;
+    gnu_ = grad_.p + 15 * nt;  // nu_tilde gradient planes follow the 15 mean-flow planes
+    ab_.sa_pre = n * (8.0 * 8 + 3 * 8.0) + double(dm_.nb) * (4 + 4 + 8 + 8 * 3 + 8 * 3);
+    ab_.sa_grad = n * 8.0 + double(g_col_.count) * (4 + 3 * 8.0) + n * 3 * 8.0;
+    ab_.sa_face = double(nf) * (4 * 2 + 8 * 5 + 8 * 4 + 8 * 4) + double(dm_.nb) * (4 + 8) + nt * (8 * 2 + 8 * 3 + 8);
+    ab_.sa_jac = double(dm_.ni) * (4 * 2 + 8 * 2 + 2 * 4.0) + n * (4 * 3 + 8 * 2) + double(sys_->nnzb()) * (4 + 4) +
+                 double(sys_->nnzb()) * 11 * ((cfg_.precision == CFDG_PREC_MIXED) ? 4.0 : 8.0);
 }
 
 void Solver::sizes(int64_t* out) const {
@@ -869,6 +949,10 @@ void Solver::init_fields() {
     for (int v5 = 0; v5 < 5; ++v5) {
         ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, 8.0 * dm_.n);
         launch_fill(U_.p + static_cast<std::size_t>(v5) * dm_.n, dm_.n, U[v5], stream_);
+    }
+    if (sa_) {  // rho * nu_tilde_inf (SpalartAllmaras::initialize, spalart_allmaras.hpp:197-198)
+        ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, 8.0 * dm_.n);
+        launch_fill(U_.p + static_cast<std::size_t>(5) * dm_.n, dm_.n, rho * sap_.nu_inf, stream_);
     }
     cuda_check(cudaGetLastError(), "init launch");
     cuda_check(cudaStreamSynchronize(stream_), "init sync");
@@ -900,6 +984,8 @@ void Solver::get_field(int field, double* out, int64_t count) {
         case CFDG_FIELD_RHS: src = b_.p; need = n * nv_; break;
         case CFDG_FIELD_MUT: src = mut_.p; need = sa_ ? nt : 0; break;
         case CFDG_FIELD_WALLDIST: src = wall_dist_.p; need = sa_ ? n : 0; break;
+        case CFDG_FIELD_NU: src = nu_.p; need = sa_ ? n : 0; break;
+        case CFDG_FIELD_NU_GRAD: src = gnu_; need = sa_ ? nt * 3 : 0; break;
         case CFDG_FIELD_JAC: {
             need = sys_->nnzb() * sys_->bs() * sys_->bs();
             if (count < need) throw Failure{CFDG_ERR_INVALID, "output buffer too small"};
@@ -917,14 +1003,24 @@ void Solver::get_field(int field, double* out, int64_t count) {
 void Solver::stage(int st) {
     switch (st) {
         case CFDG_STAGE_PRIMITIVES: {
-            ProfScope ps(&prof_, CFDG_KCAT_PRIMITIVES, stream_, 1, ab_.prim);
-            launch_primitives(dm_, df_, gas_, stream_);
+            {
+                ProfScope ps(&prof_, CFDG_KCAT_PRIMITIVES, stream_, 1, ab_.prim);
+                launch_primitives(dm_, df_, gas_, stream_);
+            }
+            if (sa_) {
+                ProfScope ps(&prof_, CFDG_KCAT_TURBULENCE, stream_, 1, ab_.sa_pre);
+                launch_sa_pre(dm_, df_, gas_, sap_, rhonu_g_.p, stream_);
+            }
             break;
         }
         case CFDG_STAGE_GRADIENT:
             if (need_grad_) {
                 ProfScope ps(&prof_, CFDG_KCAT_GRADIENT, stream_, 1, ab_.grad);
                 launch_gradient(dm_, q_.p, grad_.p, 5, stream_);
+            }
+            if (sa_) {
+                ProfScope ps(&prof_, CFDG_KCAT_GRADIENT, stream_, 1, ab_.sa_grad);
+                launch_gradient(dm_, nu_.p, gnu_, 1, stream_);
             }
             break;
         case CFDG_STAGE_LIMITER:
@@ -938,8 +1034,14 @@ void Solver::stage(int st) {
                 ProfScope ps(&prof_, CFDG_KCAT_FACE_FLUX, stream_, 1, ab_.face_flux);
                 launch_face_flux(dm_, df_, gas_, muscl_, cfg_.viscous != 0, stream_);
             }
-            ProfScope ps(&prof_, CFDG_KCAT_CELL_GATHER, stream_, 1, ab_.cell_gather);
-            launch_cell_residual(dm_, df_, stream_);
+            {
+                ProfScope ps(&prof_, CFDG_KCAT_CELL_GATHER, stream_, 1, ab_.cell_gather);
+                launch_cell_residual(dm_, df_, stream_);
+            }
+            if (sa_) {
+                ProfScope ps(&prof_, CFDG_KCAT_TURBULENCE, stream_, 2, ab_.sa_face);
+                launch_sa_sweep(dm_, df_, gas_, sap_, rhonu_g_.p, gnu_, sa_face_.p, sa_jac_.p, sa_dsrc_.p, stream_);
+            }
             break;
         }
         default: throw Failure{CFDG_ERR_INVALID, "unknown stage"};
@@ -969,11 +1071,20 @@ void Solver::assemble_jacobian() {
     js.diag = v.diag;
     js.trans = trans_.p;
     js.face_pos = face_pos_.p;
-    ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 3, ab_.jac);
-    if (cfg_.precision == CFDG_PREC_MIXED)
-        launch_jacobian<float>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values32(), bjac_.p, stream_);
-    else
-        launch_jacobian<double>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values64(), bjac_.p, stream_);
+    {
+        ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 3, ab_.jac);
+        if (cfg_.precision == CFDG_PREC_MIXED)
+            launch_jacobian<float>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values32(), bjac_.p, stream_);
+        else
+            launch_jacobian<double>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values64(), bjac_.p, stream_);
+    }
+    if (sa_) {
+        ProfScope ps(&prof_, CFDG_KCAT_TURBULENCE, stream_, 2, ab_.sa_jac);
+        if (cfg_.precision == CFDG_PREC_MIXED)
+            launch_sa_jacobian<float>(dm_, df_, js, sa_jac_.p, sa_dsrc_.p, sys_->values32(), stream_);
+        else
+            launch_sa_jacobian<double>(dm_, df_, js, sa_jac_.p, sa_dsrc_.p, sys_->values64(), stream_);
+    }
     cuda_check(cudaGetLastError(), "jacobian launch");
 }
 

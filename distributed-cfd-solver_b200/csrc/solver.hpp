@@ -220,7 +220,12 @@ private:
     DevArray<BcPatch> patches_;
     std::vector<BcPatch> patches_h_;
     // fields
-    DevArray<double> U_, q_, grad_, phi_, fflux_, res_, lam_, dt_, alpha_, nu_, rho_, mut_, sa_face_;
+    DevArray<double> U_, q_, grad_, phi_, fflux_, res_, lam_, dt_, alpha_;
+    // Spalart-Allmaras: nu_tilde, rho, mu_t (n_total), ghost rho*nu_tilde (nb),
+    // face flux + spectral increments (2 nf), face d flux / d(rho nu_tilde) (2 nf),
+    // destruction derivative (n); the nu_tilde gradient lives in grad_ planes 15..17
+    DevArray<double> nu_, rho_, mut_, rhonu_g_, sa_face_, sa_jac_, sa_dsrc_;
+    double* gnu_ = nullptr;
     // linear system
     std::unique_ptr<BsrSystem> sys_;
     DevArray<int32_t> trans_, face_pos_;
@@ -230,6 +235,7 @@ private:
     // algorithmic (unique-touch) bytes per launch of each residual-side kernel
     struct {
         double prim, grad, limiter, face_flux, cell_gather, jac, dt_rhs, state_update, norms;
+        double sa_pre, sa_grad, sa_face, sa_jac;
     } ab_{};
     void compute_alg_bytes(int64_t n_grad_edges, int64_t n_c2c, int64_t n_c2f);
     cfdg_krylov_result last_krylov_{};

@@ -97,7 +97,9 @@ enum {
     CFDG_FIELD_DU = 9,       /* last Newton update, AoS n_cells x nvars           */
     CFDG_FIELD_MUT = 10,     /* eddy viscosity, n_total (SA only)                 */
     CFDG_FIELD_WALLDIST = 11,/* wall distance, n_cells (SA only)                  */
-    CFDG_FIELD_RHS = 12      /* linear right-hand side -R, AoS n_cells x nvars    */
+    CFDG_FIELD_RHS = 12,     /* linear right-hand side -R, AoS n_cells x nvars    */
+    CFDG_FIELD_NU = 13,      /* specific nu_tilde, n_cells (SA only)              */
+    CFDG_FIELD_NU_GRAD = 14  /* nu_tilde gradient, 3 planes x n_total (SA only)  */
 };
 
 /* Pipeline stages for cfdg_solver_stage (each is one step of
@@ -114,7 +116,7 @@ enum {
 enum {
     CFDG_KCAT_PRIMITIVES = 0, CFDG_KCAT_GRADIENT = 1, CFDG_KCAT_LIMITER = 2, CFDG_KCAT_FACE_FLUX = 3,
     CFDG_KCAT_CELL_GATHER = 4, CFDG_KCAT_JACOBIAN = 5, CFDG_KCAT_LU = 6, CFDG_KCAT_SPMV = 7, CFDG_KCAT_SGS = 8,
-    CFDG_KCAT_KRYLOV = 9, CFDG_KCAT_UPDATE = 10, CFDG_KCAT_COUNT = 11
+    CFDG_KCAT_KRYLOV = 9, CFDG_KCAT_UPDATE = 10, CFDG_KCAT_TURBULENCE = 11, CFDG_KCAT_COUNT = 12
 };
 
 /* ------------------------------------------------------------- structures */

@@ -19,8 +19,21 @@
 
 typedef struct {
     int kind;
+    int sa_kind; /* SpalartAllmaras::zone_kind: 0 wall, 1 inflow, 2 outflow, 3 symmetry */
     double qfix[5], p_out, tmp_grad, far_p, far_T, far_u, far_v, far_w;
 } bcp_t;
+
+/* Spalart & Allmaras (1994) constants (spalart_allmaras.hpp:85-93). */
+#define SA_CB1 0.1355
+#define SA_CB2 0.622
+#define SA_SIGMA (2.0 / 3.0)
+#define SA_KAPPA 0.41
+#define SA_CW2 0.3
+#define SA_CW3 2.0
+#define SA_CV1 7.1
+#define SA_CW1 (SA_CB1 / (SA_KAPPA * SA_KAPPA) + (1.0 + SA_CB2) / SA_SIGMA)
+#define SA_SBAR_FLOOR 1.0e-10
+#define SA_MIN_WALL_DIST 1.0e-10
 
 struct oracle_solver {
     cfdg_mesh_host m;
@@ -36,6 +49,10 @@ struct oracle_solver {
     int32_t *rp, *cols, *diag;
     int64_t nnzb;
     double *U, *q, *grad, *phi, *res, *lam, *alpha, *vals;
+    /* Spalart-Allmaras */
+    int sa;
+    double nu_inf, rhonu_inf;
+    double *dist, *nu, *rho, *mut, *gnu, *mdot, *rhonu_g;
 };
 
 static void* xcalloc(size_t n, size_t s) { return calloc(n ? n : 1, s); }
@@ -227,11 +244,14 @@ static void euler_jac(const oracle_solver* s, const double* U, double nx, double
 /* ViscousFlux::face_flux (fluxes/viscous.hpp:90-175): cell-centre states,
  * averaged gradients, over-relaxed normal derivative. */
 static double viscous(const oracle_solver* s, int f, const double* qL, const double* qR, const double* gL,
-                      const double* gR, double nx, double ny, double nz, double A, double* Fv) {
+                      const double* gR, double mutL, double mutR, double nx, double ny, double nz, double A,
+                      double* Fv) {
     const double pf = 0.5 * (qL[0] + qR[0]), uf = 0.5 * (qL[1] + qR[1]), vf = 0.5 * (qL[2] + qR[2]);
     const double wf = 0.5 * (qL[3] + qR[3]), Tf = 0.5 * (qL[4] + qR[4]);
-    const double mu = sutherland(Tf);
-    const double k = mu * s->cp / s->cfg.prandtl;
+    const double mu_lam = sutherland(Tf);
+    const double mu_t = 0.5 * (mutL + mutR);
+    const double mu = mu_lam + mu_t;
+    const double k = (mu_lam * s->cp) / s->cfg.prandtl + (mu_t * s->cp) / s->cfg.prandtl_turb;
     const double id = s->finv_d[f];
     const double cx = nx - s->fdx[f] * id, cy = ny - s->fdy[f] * id, cz = nz - s->fdz[f] * id;
     double g[12];
@@ -256,11 +276,13 @@ static double viscous(const oracle_solver* s, int f, const double* qL, const dou
 }
 
 /* ViscousFlux::face_flux_jacobian, thin layer (fluxes/viscous.hpp:280-360). */
-static void viscous_jac(const oracle_solver* s, int f, const double* qL, const double* qR, double A, double* J) {
+static void viscous_jac(const oracle_solver* s, int f, const double* qL, const double* qR, double mutL, double mutR,
+                        double A, double* J) {
     const double pf = 0.5 * (qL[0] + qR[0]), uf = 0.5 * (qL[1] + qR[1]), vf = 0.5 * (qL[2] + qR[2]);
     const double wf = 0.5 * (qL[3] + qR[3]), Tf = 0.5 * (qL[4] + qR[4]);
     const double rho = pf / (s->R * Tf), ir = 1.0 / rho, irc = 1.0 / (rho * s->cv);
-    const double mu = sutherland(Tf), k = mu * s->cp / s->cfg.prandtl;
+    const double mu_lam = sutherland(Tf), mu_t = 0.5 * (mutL + mutR), mu = mu_lam + mu_t;
+    const double k = (mu_lam * s->cp) / s->cfg.prandtl + (mu_t * s->cp) / s->cfg.prandtl_turb;
     const double Cm = mu * s->finv_d[f] * A, Cl = k * s->finv_d[f] * A;
     const double V2 = uf * uf + vf * vf + wf * wf;
     memset(J, 0, 25 * sizeof(double));
@@ -479,6 +501,49 @@ static void lsq_setup(oracle_solver* s) {
     }
 }
 
+/* MeshAuxGeometry::add_wall_distance with the face-neighbour stencil
+ * (src/mesh/aux_geometry.cpp:541-696): seed wall-adjacent cells with the
+ * owner-to-face-centroid distance, then forward/backward Gauss-Seidel
+ * relaxation d_c = min(d_c, d_j + |x_c - x_j|) until the largest relative
+ * change is <= tol or max_sweeps passes. */
+static void wall_distance(oracle_solver* s, int max_sweeps, double tol) {
+    const cfdg_mesh_host* m = &s->m;
+    const int n = s->n;
+    for (int c = 0; c < n; ++c) s->dist[c] = 1.0e30;
+    for (int f = s->ni; f < s->nf; ++f) {
+        if (s->bcp[m->face_patch[f]].sa_kind != 0) continue;
+        const int c0 = m->face_owner[f];
+        const double ex = m->face_centroid_x[f] - m->cell_centroid_x[c0];
+        const double ey = m->face_centroid_y[f] - m->cell_centroid_y[c0];
+        const double ez = m->face_centroid_z[f] - m->cell_centroid_z[c0];
+        const double d = sqrt(ex * ex + ey * ey + ez * ez);
+        if (d < s->dist[c0]) s->dist[c0] = d;
+    }
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+        double max_rel = 0.0;
+        for (int pass = 0; pass < 2; ++pass)
+            for (int k = 0; k < n; ++k) {
+                const int c = pass == 0 ? k : n - 1 - k;
+                const double d0 = s->dist[c];
+                double dn = d0;
+                for (int j = s->c2c_off[c]; j < s->c2c_off[c + 1]; ++j) {
+                    const int o = s->c2c[j];
+                    const double dx = m->cell_centroid_x[o] - m->cell_centroid_x[c];
+                    const double dy = m->cell_centroid_y[o] - m->cell_centroid_y[c];
+                    const double dz = m->cell_centroid_z[o] - m->cell_centroid_z[c];
+                    const double cand = s->dist[o] + sqrt(dx * dx + dy * dy + dz * dz);
+                    dn = cand < dn ? cand : dn;
+                }
+                if (dn < d0) {
+                    const double rel = (d0 - dn) / (d0 > 1.0e-12 ? d0 : 1.0e-12);
+                    if (rel > max_rel) max_rel = rel;
+                    s->dist[c] = dn;
+                }
+            }
+        if (max_rel <= tol) break;
+    }
+}
+
 int oracle_create(const cfdg_mesh_host* m, const cfdg_config* cfg, const cfdg_bc_desc* bcs, int nbc,
                   oracle_solver** out) {
     oracle_solver* s = (oracle_solver*)calloc(1, sizeof(oracle_solver));
@@ -493,13 +558,17 @@ int oracle_create(const cfdg_mesh_host* m, const cfdg_config* cfg, const cfdg_bc
     s->ni = m->n_inner_faces;
     s->nb = s->nf - s->ni;
     s->nt = s->n + s->nb;
-    s->nv = 5;
+    s->sa = cfg->turbulence == 1;
+    s->nv = s->sa ? 6 : 5;
     s->muscl = cfg->reconstruction == CFDG_RECON_MUSCL;
     s->visc = cfg->viscous != 0;
     s->need_grad = s->muscl || s->visc;
     s->n_patch = m->n_patches > 0 ? m->n_patches : 1;
     s->bcp = (bcp_t*)xcalloc((size_t)s->n_patch, sizeof(bcp_t));
-    for (int p = 0; p < s->n_patch; ++p) s->bcp[p].kind = -1;
+    for (int p = 0; p < s->n_patch; ++p) {
+        s->bcp[p].kind = -1;
+        s->bcp[p].sa_kind = 3;
+    }
     /* BoundaryManager::register_all parameter resolution (bc_manager.hpp:223-329) */
     for (int i = 0; i < nbc; ++i) {
         const cfdg_bc_desc* d = &bcs[i];
@@ -507,6 +576,17 @@ int oracle_create(const cfdg_mesh_host* m, const cfdg_config* cfg, const cfdg_bc
         bcp_t* P = &s->bcp[d->patch_id];
         memset(P, 0, sizeof(*P));
         P->kind = d->type;
+        /* SpalartAllmaras::zone_kind (spalart_allmaras.hpp:458-475) */
+        switch (d->type) {
+            case CFDG_BC_NO_SLIP_WALL:
+            case CFDG_BC_NO_SLIP_WALL_HEAT_FLUX: P->sa_kind = 0; break;
+            case CFDG_BC_SUPERSONIC_INLET:
+            case CFDG_BC_SUBSONIC_INLET:
+            case CFDG_BC_FARFIELD: P->sa_kind = 1; break;
+            case CFDG_BC_SUPERSONIC_OUTLET:
+            case CFDG_BC_SUBSONIC_OUTLET: P->sa_kind = 2; break;
+            default: P->sa_kind = 3; break;
+        }
         double st[5];
         switch (d->type) {
             case CFDG_BC_SUPERSONIC_INLET:
@@ -594,15 +674,29 @@ int oracle_create(const cfdg_mesh_host* m, const cfdg_config* cfg, const cfdg_bc
         for (int k = s->rp[c]; k < s->rp[c + 1]; ++k)
             if (s->cols[k] == c) s->diag[c] = k;
     }
-    const size_t nt = (size_t)s->nt;
-    s->U = (double*)xcalloc(5 * (size_t)n, 8);
+    const size_t nt = (size_t)s->nt, nv = (size_t)s->nv;
+    s->U = (double*)xcalloc(nv * (size_t)n, 8);
     s->q = (double*)xcalloc(5 * nt, 8);
     s->grad = (double*)xcalloc(15 * nt, 8);
     s->phi = (double*)xcalloc(5 * (size_t)n, 8);
-    s->res = (double*)xcalloc(5 * (size_t)n, 8);
+    s->res = (double*)xcalloc(nv * (size_t)n, 8);
     s->lam = (double*)xcalloc((size_t)n, 8);
     s->alpha = (double*)xcalloc((size_t)n, 8);
-    s->vals = (double*)xcalloc((size_t)s->nnzb * 25, 8);
+    s->vals = (double*)xcalloc((size_t)s->nnzb * nv * nv, 8);
+    if (s->sa) {
+        s->dist = (double*)xcalloc((size_t)n, 8);
+        s->nu = (double*)xcalloc(nt, 8);
+        s->rho = (double*)xcalloc(nt, 8);
+        s->mut = (double*)xcalloc(nt, 8);
+        s->gnu = (double*)xcalloc(3 * nt, 8);
+        s->mdot = (double*)xcalloc((size_t)s->nf, 8);
+        s->rhonu_g = (double*)xcalloc((size_t)s->nb, 8);
+        wall_distance(s, 1000000, 0.0); /* to the exact graph fixed point */
+        /* SpalartAllmaras::initialize freestream values (spalart_allmaras.hpp:193-198) */
+        const double T_inf = cfg->init_p / (cfg->init_rho * s->R);
+        s->nu_inf = cfg->nu_inf_ratio * sutherland(T_inf) / cfg->init_rho;
+        s->rhonu_inf = cfg->init_rho * s->nu_inf;
+    }
     *out = s;
     return 0;
 }
@@ -611,7 +705,7 @@ void oracle_destroy(oracle_solver* s) {
     if (!s) return;
     void* p[] = {s->bcp, s->c2f_off, s->c2f, s->c2c_off, s->c2c, s->g_off, s->g_col, s->g_wx, s->g_wy, s->g_wz,
                  s->fdx, s->fdy, s->fdz, s->finv_d, s->rp, s->cols, s->diag, s->U, s->q, s->grad, s->phi, s->res,
-                 s->lam, s->alpha, s->vals};
+                 s->lam, s->alpha, s->vals, s->dist, s->nu, s->rho, s->mut, s->gnu, s->mdot, s->rhonu_g};
     for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); ++i) free(p[i]);
     free(s);
 }
@@ -626,11 +720,125 @@ int oracle_structure(const oracle_solver* s, int32_t* row_ptr, int32_t* cols) {
 }
 
 void oracle_set_state(oracle_solver* s, const double* U, int64_t ld) {
-    for (int v = 0; v < 5; ++v) memcpy(s->U + (size_t)v * s->n, U + v * ld, sizeof(double) * (size_t)s->n);
+    for (int v = 0; v < s->nv; ++v) memcpy(s->U + (size_t)v * s->n, U + v * ld, sizeof(double) * (size_t)s->n);
 }
 
 void oracle_get_state(const oracle_solver* s, double* U, int64_t ld) {
-    for (int v = 0; v < 5; ++v) memcpy(U + v * ld, s->U + (size_t)v * s->n, sizeof(double) * (size_t)s->n);
+    for (int v = 0; v < s->nv; ++v) memcpy(U + v * ld, s->U + (size_t)v * s->n, sizeof(double) * (size_t)s->n);
+}
+
+/* Averaged + skew-corrected nu_tilde face gradient
+ * (SpalartAllmaras::face_gradient, spalart_allmaras.hpp:486-508). */
+static void sa_face_gradient(const oracle_solver* s, int f, int cl, double nul, int cr, double nur, double* gn) {
+    const size_t nt = (size_t)s->nt;
+    const double dx = s->fdx[f], dy = s->fdy[f], dz = s->fdz[f];
+    gn[0] = 0.5 * (s->gnu[cl] + s->gnu[cr]);
+    gn[1] = 0.5 * (s->gnu[nt + cl] + s->gnu[nt + cr]);
+    gn[2] = 0.5 * (s->gnu[2 * nt + cl] + s->gnu[2 * nt + cr]);
+    const double gd = gn[0] * dx + gn[1] * dy + gn[2] * dz;
+    const double id = s->finv_d[f];
+    const double corr = ((nur - nul) - gd) * id * id;
+    gn[0] += corr * dx;
+    gn[1] += corr * dy;
+    gn[2] += corr * dz;
+}
+
+/* Spalart-Allmaras convection + diffusion face sweep and cell sources
+ * (SpalartAllmaras::face_sweep / cell_sources, spalart_allmaras.hpp:291-432)
+ * with the standard SA-1994 signs: the diffusive flux enters the residual
+ * with a minus sign (the reference adds it), the cb2 term is a source
+ * (the reference adds it to the residual), S = sqrt(2 S_ij S_ij) with full
+ * weight on the shear terms (the reference halves them) and
+ * f_w = g ((1 + cw3^6) / (g^6 + cw3^6))^(1/6) (the reference drops cw3^6
+ * from the denominator); at walls and symmetry planes the boundary face is
+ * never an inflow (the reference tests the sign of a round-off mass flux). */
+/* f_w of cell c from the stored nu_tilde, wall distance and gradients. */
+static double sa_fw_core(const oracle_solver* s, int c, double* sbar_out) {
+    const size_t nt = (size_t)s->nt;
+    const double rho = s->rho[c], nu = s->nu[c];
+    const double d = fmax(s->dist[c], SA_MIN_WALL_DIST), id2 = 1.0 / (d * d);
+    const double* gr = s->grad;
+    const double ux = gr[3 * nt + c], uy = gr[4 * nt + c], uz = gr[5 * nt + c];
+    const double vx = gr[6 * nt + c], vy = gr[7 * nt + c], vz = gr[8 * nt + c];
+    const double wx = gr[9 * nt + c], wy = gr[10 * nt + c], wz = gr[11 * nt + c];
+    const double sxy = uy + vx, sxz = uz + wx, syz = vz + wy;
+    const double s2 = 2.0 * (ux * ux + vy * vy + wz * wz) + sxy * sxy + sxz * sxz + syz * syz;
+    const double S = sqrt(fmax(s2, 0.0));
+    const double nu_lam = sutherland(s->q[4 * nt + c]) / rho;
+    const double chi = nu / nu_lam, chi3 = chi * chi * chi;
+    const double fv1 = chi3 / (chi3 + SA_CV1 * SA_CV1 * SA_CV1);
+    const double fv2 = 1.0 - chi / (1.0 + chi * fv1);
+    const double ik2 = 1.0 / (SA_KAPPA * SA_KAPPA);
+    const double sbar = fmax(S + nu * fv2 * ik2 * id2, SA_SBAR_FLOOR);
+    double r = nu / (sbar * SA_KAPPA * SA_KAPPA * d * d);
+    r = fmin(fmax(r, 0.0), 10.0);
+    const double r2 = r * r, r6 = r2 * r2 * r2;
+    const double g = r + SA_CW2 * (r6 - r);
+    const double g2 = g * g, g6 = g2 * g2 * g2;
+    const double cw3_6 = SA_CW3 * SA_CW3 * SA_CW3 * SA_CW3 * SA_CW3 * SA_CW3;
+    if (sbar_out) *sbar_out = sbar;
+    return g * pow((1.0 + cw3_6) / (g6 + cw3_6), 1.0 / 6.0);
+}
+
+static double sa_fw(const oracle_solver* s, int c) { return sa_fw_core(s, c, NULL); }
+
+static void sa_residual(oracle_solver* s) {
+    const cfdg_mesh_host* m = &s->m;
+    const int n = s->n, nt = s->nt, ni = s->ni, nf = s->nf;
+    double* res = s->res + (size_t)5 * n;
+    const double is = 1.0 / SA_SIGMA;
+    memset(res, 0, sizeof(double) * (size_t)n);
+    for (int f = 0; f < nf; ++f) {
+        const int inner = f < ni;
+        const int c0 = m->face_owner[f], b = f - ni;
+        const int c1 = inner ? m->face_neigh[f] : n + b;
+        const double nx = m->face_normal_x[f], ny = m->face_normal_y[f], nz = m->face_normal_z[f], A = m->face_area[f];
+        const double mf = s->mdot[f];
+        double gn[3];
+        if (inner) {
+            const double nu_up = (mf >= 0.0) ? s->nu[c0] : s->nu[c1];
+            sa_face_gradient(s, f, c0, s->nu[c0], c1, s->nu[c1], gn);
+            const double Tf = 0.5 * (s->q[4 * (size_t)nt + c0] + s->q[4 * (size_t)nt + c1]);
+            const double mu_f = sutherland(Tf);
+            const double rho_f = 0.5 * (s->rho[c0] + s->rho[c1]);
+            const double nu_f = 0.5 * (s->nu[c0] + s->nu[c1]);
+            const double coef = is * (mu_f + rho_f * nu_f);
+            const double fd = coef * (gn[0] * nx + gn[1] * ny + gn[2] * nz) * A;
+            const double flux = mf * nu_up - fd;
+            res[c0] += flux;
+            res[c1] -= flux;
+            const double w = fabs(mf) / rho_f + 2.0 * is * (mu_f + rho_f * nu_f) / rho_f * A * s->finv_d[f];
+            s->lam[c0] += w;
+            s->lam[c1] += w;
+        } else {
+            /* walls and symmetry planes carry no mass flux: their m is
+             * round-off, so only inflow/outflow patches switch on its sign */
+            const int kind = s->bcp[m->face_patch[f]].sa_kind;
+            const int inflow = (kind == 1 || kind == 2) && mf < 0.0;
+            const double pg = s->q[0 * (size_t)nt + c1], Tg = s->q[4 * (size_t)nt + c1];
+            const double rho_g = pg / (s->R * Tg);
+            const double nu_g = inflow ? s->nu_inf : s->rhonu_g[b] / rho_g;
+            const double nu_up = inflow ? s->nu_inf : s->nu[c0];
+            sa_face_gradient(s, f, c0, s->nu[c0], c1, nu_g, gn);
+            const double Tf = 0.5 * (s->q[4 * (size_t)nt + c0] + Tg);
+            const double mu_f = sutherland(Tf);
+            const double rho_f = 0.5 * (s->rho[c0] + rho_g);
+            const double coef = is * (mu_f + rho_f * 0.5 * (s->nu[c0] + nu_g));
+            const double fd = coef * (gn[0] * nx + gn[1] * ny + gn[2] * nz) * A;
+            res[c0] += mf * nu_up - fd;
+        }
+    }
+    for (int c = 0; c < n; ++c) {
+        const double rho = s->rho[c], nu = s->nu[c];
+        const double d = fmax(s->dist[c], SA_MIN_WALL_DIST), id2 = 1.0 / (d * d);
+        double sbar;
+        const double fw = sa_fw_core(s, c, &sbar);
+        const double P = SA_CB1 * sbar * rho * nu;
+        const double D = SA_CW1 * fw * rho * nu * nu * id2;
+        const double gnx = s->gnu[c], gny = s->gnu[(size_t)nt + c], gnz = s->gnu[2 * (size_t)nt + c];
+        const double cb2 = (SA_CB2 / SA_SIGMA) * rho * (gnx * gnx + gny * gny + gnz * gnz);
+        res[c] += m->cell_volume[c] * (D - P - cb2);
+    }
 }
 
 /* ------------------------------------------------------- residual pipeline */
@@ -657,6 +865,35 @@ static void residual(oracle_solver* s) {
         for (int v = 0; v < 5; ++v) qi[v] = q[v * nt + c0];
         ghost_values(s, &s->bcp[m->face_patch[f]], qi, nx, ny, nz, rcfn, qg);
         for (int v = 0; v < 5; ++v) q[v * nt + g] = qg[v];
+    }
+    if (s->sa) {
+        /* SpalartAllmaras::apply_bcs (spalart_allmaras.hpp:234-257): ghost rho*nu_tilde */
+        for (int f = ni; f < nf; ++f) {
+            const int c0 = m->face_owner[f], b = f - ni, g = n + b;
+            const bcp_t* P = &s->bcp[m->face_patch[f]];
+            const double rn0 = s->U[(size_t)5 * n + c0];
+            if (P->sa_kind == 0) s->rhonu_g[b] = -rn0;
+            else if (P->sa_kind == 1) s->rhonu_g[b] = (q[0 * nt + g] / (s->R * q[4 * nt + g])) * s->nu_inf;
+            else s->rhonu_g[b] = rn0;
+        }
+        /* SpalartAllmaras::pre_sweep (spalart_allmaras.hpp:263-282): density,
+         * specific nu_tilde and eddy viscosity on cells; zero eddy viscosity on
+         * BC ghosts */
+        for (int c = 0; c < n; ++c) {
+            const double rho = q[0 * nt + c] / (s->R * q[4 * nt + c]);
+            const double nu = s->U[(size_t)5 * n + c] / rho;
+            s->rho[c] = rho;
+            s->nu[c] = nu;
+            const double nu_lam = sutherland(q[4 * nt + c]) / rho;
+            const double chi = nu / nu_lam, chi3 = chi * chi * chi;
+            const double fv1 = chi3 / (chi3 + SA_CV1 * SA_CV1 * SA_CV1);
+            s->mut[c] = rho * nu * fv1;
+        }
+        for (int g = n; g < nt; ++g) {
+            s->mut[g] = 0.0;
+            s->rho[g] = 0.0;
+            s->nu[g] = 0.0;
+        }
     }
     if (s->need_grad) {
         /* 5: LSQ gradients (apply_kernel_lsq*, gradient_operator.cpp:340-391,549-599) */
@@ -729,6 +966,28 @@ static void residual(oracle_solver* s) {
             }
             for (int v = 0; v < 5; ++v)
                 for (int d = 0; d < 3; ++d) s->grad[(3 * v + d) * (size_t)nt + g] = gg[v][d];
+        }
+    }
+    if (s->sa) {
+        /* nu_tilde gradient with the solver's least-squares stencil on cells,
+         * BC ghost planes mirror the owner with a sign flip at walls
+         * (SpalartAllmaras::compute_gradients, spalart_allmaras.hpp:212-229) */
+        for (int c = 0; c < n; ++c) {
+            double gx = 0, gy = 0, gz = 0;
+            for (int j = s->g_off[c]; j < s->g_off[c + 1]; ++j) {
+                const double d = s->nu[s->g_col[j]] - s->nu[c];
+                gx += s->g_wx[j] * d;
+                gy += s->g_wy[j] * d;
+                gz += s->g_wz[j] * d;
+            }
+            s->gnu[c] = gx;
+            s->gnu[(size_t)nt + c] = gy;
+            s->gnu[2 * (size_t)nt + c] = gz;
+        }
+        for (int f = ni; f < nf; ++f) {
+            const int c0 = m->face_owner[f], g = n + (f - ni);
+            const double sg = (s->bcp[m->face_patch[f]].sa_kind == 0) ? -1.0 : 1.0;
+            for (int p = 0; p < 3; ++p) s->gnu[(size_t)p * nt + g] = sg * s->gnu[(size_t)p * nt + c0];
         }
     }
     if (s->muscl) {
@@ -807,6 +1066,7 @@ static void residual(oracle_solver* s) {
         prim2cons(s, qL, UL);
         prim2cons(s, qR, UR);
         hllc(s, UL, UR, nx, ny, nz, A, F, &smax);
+        if (s->sa) s->mdot[f] = F[0];
         double lf = A * smax;
         if (s->visc) {
             double qcL[5], qcR[5], gL[12], gR[12], Fv[5];
@@ -819,7 +1079,8 @@ static void residual(oracle_solver* s) {
                     gL[(v - 1) * 3 + d] = s->grad[(3 * v + d) * (size_t)nt + c0];
                     gR[(v - 1) * 3 + d] = s->grad[(3 * v + d) * (size_t)nt + c1];
                 }
-            lf += viscous(s, f, qcL, qcR, gL, gR, nx, ny, nz, A, Fv);
+            const double mutL = s->sa ? s->mut[c0] : 0.0, mutR = s->sa ? s->mut[c1] : 0.0;
+            lf += viscous(s, f, qcL, qcR, gL, gR, mutL, mutR, nx, ny, nz, A, Fv);
             for (int v = 1; v < 5; ++v) F[v] += Fv[v];
         }
         for (int v = 0; v < 5; ++v) {
@@ -829,6 +1090,7 @@ static void residual(oracle_solver* s) {
         s->lam[c0] += lf;
         if (inner) s->lam[c1] += lf;
     }
+    if (s->sa) sa_residual(s);
 }
 
 void oracle_stages(oracle_solver* s, double* q, double* grad, double* phi, double* res, double* lam) {
@@ -837,7 +1099,7 @@ void oracle_stages(oracle_solver* s, double* q, double* grad, double* phi, doubl
     if (q) memcpy(q, s->q, sizeof(double) * 5 * nt);
     if (grad) memcpy(grad, s->grad, sizeof(double) * 15 * nt);
     if (phi) memcpy(phi, s->phi, sizeof(double) * 5 * n);
-    if (res) memcpy(res, s->res, sizeof(double) * 5 * n);
+    if (res) memcpy(res, s->res, sizeof(double) * (size_t)s->nv * n);
     if (lam) memcpy(lam, s->lam, sizeof(double) * n);
 }
 
@@ -853,15 +1115,24 @@ static int bsr_pos(const oracle_solver* s, int row, int col) {
 }
 
 /* compute_dt (solver.hpp:256-287) then JacobianKernel::apply
- * (jacobian_kernel.hpp:74-270). */
+ * (jacobian_kernel.hpp:74-270): first-order Picard blocks from cell-centre
+ * states, alpha on the diagonal.  With Spalart-Allmaras the blocks are 6x6:
+ * the mean-flow 5x5 part as above, and the nu_tilde row/column carries only
+ * the d/d(rho nu_tilde) entry (new math, the reference module has no
+ * Jacobian): upwind convection m+/rho_L, m-/rho_R; thin-layer diffusion
+ * +-coef A/|d|/rho; at boundary faces the ghost's dependence on the owner
+ * (wall -1/rho_g, symmetry/outflow +1/rho_g, inflow 0); the destruction
+ * derivative V 2 cw1 fw nu/d^2 on the diagonal.  Mean flow and turbulence
+ * are not coupled in the Jacobian (Picard). */
 static void jacobian(oracle_solver* s, double cfl) {
     const cfdg_mesh_host* m = &s->m;
-    const int n = s->n, nt = s->nt, ni = s->ni, nf = s->nf;
+    const int n = s->n, nt = s->nt, ni = s->ni, nf = s->nf, bs = s->nv, b2 = bs * bs;
     for (int c = 0; c < n; ++c) {
         const double l = fmax(s->lam[c], 1e-14);
         s->alpha[c] = l * (1.0 / cfl) + m->cell_volume[c] * 0.0;
     }
-    memset(s->vals, 0, sizeof(double) * 25 * (size_t)s->nnzb);
+    memset(s->vals, 0, sizeof(double) * (size_t)b2 * (size_t)s->nnzb);
+    const double is = 1.0 / SA_SIGMA;
     for (int f = 0; f < nf; ++f) {
         const int inner = f < ni;
         const int c0 = m->face_owner[f], c1 = inner ? m->face_neigh[f] : n + (f - ni);
@@ -885,37 +1156,83 @@ static void jacobian(oracle_solver* s, double cfl) {
             dFR[i * 6] -= 0.5 * smax * A;
         }
         if (s->visc) {
-            viscous_jac(s, f, qL, qR, A, Jv);
+            const double mutL = s->sa ? s->mut[c0] : 0.0;
+            const double mutR = (s->sa && inner) ? s->mut[c1] : 0.0;
+            viscous_jac(s, f, qL, qR, mutL, mutR, A, Jv);
             for (int i = 0; i < 25; ++i) {
                 dFL[i] += Jv[i];
                 dFR[i] += -Jv[i];
             }
         }
-        double* a00 = s->vals + 25 * (size_t)s->diag[c0];
-        if (inner) {
-            double* a01 = s->vals + 25 * (size_t)bsr_pos(s, c0, c1);
-            double* a11 = s->vals + 25 * (size_t)s->diag[c1];
-            double* a10 = s->vals + 25 * (size_t)bsr_pos(s, c1, c0);
-            for (int i = 0; i < 25; ++i) {
-                a00[i] += dFL[i];
-                a01[i] += dFR[i];
+        double sL = 0.0, sR = 0.0; /* d F_nu / d (rho nu_tilde) of the two sides */
+        if (s->sa) {
+            const double mf = s->mdot[f], id = s->finv_d[f];
+            if (inner) {
+                const double Tf = 0.5 * (qL[4] + qR[4]);
+                const double rho_f = 0.5 * (s->rho[c0] + s->rho[c1]);
+                const double nu_f = 0.5 * (s->nu[c0] + s->nu[c1]);
+                const double cd = is * (sutherland(Tf) + rho_f * nu_f) * A * id;
+                sL = (fmax(mf, 0.0) + cd) / s->rho[c0];
+                sR = (fmin(mf, 0.0) - cd) / s->rho[c1];
+            } else {
+                const int b = f - ni;
+                const bcp_t* P = &s->bcp[m->face_patch[f]];
+                const double rho_g = qR[0] / (s->R * qR[4]);
+                const int inflow = (P->sa_kind == 1 || P->sa_kind == 2) && mf < 0.0;
+                const double nu_g = inflow ? s->nu_inf : s->rhonu_g[b] / rho_g;
+                const double Tf = 0.5 * (qL[4] + qR[4]);
+                const double rho_f = 0.5 * (s->rho[c0] + rho_g);
+                const double cd = is * (sutherland(Tf) + rho_f * 0.5 * (s->nu[c0] + nu_g)) * A * id;
+                double dg = 0.0; /* d nu_g / d (rho nu_tilde)_owner */
+                if (!inflow) dg = (P->sa_kind == 0) ? -1.0 / rho_g : (P->sa_kind == 1 ? 0.0 : 1.0 / rho_g);
+                sL = (inflow ? 0.0 : mf / s->rho[c0]) + cd * (1.0 / s->rho[c0] - dg);
             }
-            for (int i = 0; i < 25; ++i) {
-                a11[i] -= dFR[i];
-                a10[i] -= dFL[i];
+        }
+        double* a00 = s->vals + (size_t)b2 * s->diag[c0];
+        if (inner) {
+            double* a01 = s->vals + (size_t)b2 * bsr_pos(s, c0, c1);
+            double* a11 = s->vals + (size_t)b2 * s->diag[c1];
+            double* a10 = s->vals + (size_t)b2 * bsr_pos(s, c1, c0);
+            for (int r = 0; r < 5; ++r)
+                for (int k = 0; k < 5; ++k) {
+                    a00[r * bs + k] += dFL[r * 5 + k];
+                    a01[r * bs + k] += dFR[r * 5 + k];
+                }
+            for (int r = 0; r < 5; ++r)
+                for (int k = 0; k < 5; ++k) {
+                    a11[r * bs + k] -= dFR[r * 5 + k];
+                    a10[r * bs + k] -= dFL[r * 5 + k];
+                }
+            if (s->sa) {
+                a00[35] += sL;
+                a01[35] += sR;
+                a11[35] -= sR;
+                a10[35] -= sL;
             }
         } else {
-            for (int i = 0; i < 25; ++i) a00[i] += dFL[i];
+            for (int r = 0; r < 5; ++r)
+                for (int k = 0; k < 5; ++k) a00[r * bs + k] += dFL[r * 5 + k];
+            if (s->sa) a00[35] += sL;
         }
     }
-    for (int c = 0; c < n; ++c)
-        for (int i = 0; i < 5; ++i) s->vals[25 * (size_t)s->diag[c] + i * 6] += s->alpha[c];
+    for (int c = 0; c < n; ++c) {
+        double* d = s->vals + (size_t)b2 * s->diag[c];
+        for (int i = 0; i < 5; ++i) d[i * (bs + 1)] += s->alpha[c];
+        if (s->sa) {
+            const double rho = s->rho[c], nu = s->nu[c];
+            const double dd = fmax(s->dist[c], SA_MIN_WALL_DIST);
+            const double fw = sa_fw(s, c);
+            const double id2 = 1.0 / (dd * dd);
+            d[35] += m->cell_volume[c] * 2.0 * SA_CW1 * fw * nu * id2 + s->alpha[c];
+            (void)rho;
+        }
+    }
 }
 
 void oracle_jacobian(oracle_solver* s, double cfl, double* alpha, double* values) {
     jacobian(s, cfl);
     if (alpha) memcpy(alpha, s->alpha, sizeof(double) * (size_t)s->n);
-    if (values) memcpy(values, s->vals, sizeof(double) * 25 * (size_t)s->nnzb);
+    if (values) memcpy(values, s->vals, sizeof(double) * (size_t)s->nv * s->nv * (size_t)s->nnzb);
 }
 
 /* ----------------------------------------------------------- linear algebra */
@@ -1189,38 +1506,44 @@ int oracle_bicgstab(int n, int bs, const int32_t* rp, const int32_t* cols, const
 }
 
 /* ---------------------------------------------------------------- Newton */
-/* BackwardEuler::advance (time/implicit_euler.hpp:34-92). */
+/* BackwardEuler::advance (time/implicit_euler.hpp:34-92); with
+ * Spalart-Allmaras the sixth variable is updated in the same solve and
+ * clamped at zero (SpalartAllmaras::post_stage, spalart_allmaras.hpp:435-441). */
 int oracle_newton_step(oracle_solver* s, double cfl, double* l2, int* krylov) {
-    const int n = s->n;
+    const int n = s->n, bs = s->nv;
     residual(s);
     jacobian(s, cfl);
-    const size_t N = (size_t)n * 5;
+    const size_t N = (size_t)n * bs;
     double* b = (double*)xcalloc(N, 8);
     double* du = (double*)xcalloc(N, 8);
     for (int c = 0; c < n; ++c)
-        for (int v = 0; v < 5; ++v) b[(size_t)c * 5 + v] = -s->res[(size_t)v * n + c];
+        for (int v = 0; v < bs; ++v) b[(size_t)c * bs + v] = -s->res[(size_t)v * n + c];
     int it = 0, st = 2;
     double r0, rf;
     const cfdg_config* cfg = &s->cfg;
     if (cfg->precond == CFDG_PC_SGS) {
         sgs_t P;
-        if (!sgs_setup(&P, n, 5, s->rp, s->cols, s->vals, cfg->sgs_sweeps > 0 ? cfg->sgs_sweeps : 1)) {
+        if (!sgs_setup(&P, n, bs, s->rp, s->cols, s->vals, cfg->sgs_sweeps > 0 ? cfg->sgs_sweeps : 1)) {
             sgs_free(&P);
             free(b);
             free(du);
             return -1;
         }
-        bicgstab_core(n, 5, s->rp, s->cols, s->vals, &P, cfg->lin_rel_tol, cfg->lin_abs_tol, cfg->lin_max_iterations,
-                      du, b, &it, &st, &r0, &rf);
+        bicgstab_core(n, bs, s->rp, s->cols, s->vals, &P, cfg->lin_rel_tol, cfg->lin_abs_tol,
+                      cfg->lin_max_iterations, du, b, &it, &st, &r0, &rf);
         sgs_free(&P);
     } else {
-        bicgstab_core(n, 5, s->rp, s->cols, s->vals, NULL, cfg->lin_rel_tol, cfg->lin_abs_tol,
+        bicgstab_core(n, bs, s->rp, s->cols, s->vals, NULL, cfg->lin_rel_tol, cfg->lin_abs_tol,
                       cfg->lin_max_iterations, du, b, &it, &st, &r0, &rf);
     }
-    for (int v = 0; v < 5; ++v)
-        for (int c = 0; c < n; ++c) s->U[(size_t)v * n + c] += du[(size_t)c * 5 + v];
+    for (int v = 0; v < bs; ++v)
+        for (int c = 0; c < n; ++c) {
+            double x = s->U[(size_t)v * n + c] + du[(size_t)c * bs + v];
+            if (v == 5 && x < 0.0) x = 0.0;
+            s->U[(size_t)v * n + c] = x;
+        }
     /* residual_norms (solver.hpp:740-756) of the evaluated R(U) */
-    for (int v = 0; v < 5; ++v) {
+    for (int v = 0; v < bs; ++v) {
         double acc = 0.0;
         for (int c = 0; c < n; ++c) acc += s->res[(size_t)v * n + c] * s->res[(size_t)v * n + c];
         l2[v] = sqrt(acc / (double)(n > 0 ? n : 1));
@@ -1232,4 +1555,13 @@ int oracle_newton_step(oracle_solver* s, double cfl, double* l2, int* krylov) {
     free(b);
     free(du);
     return 0;
+}
+
+void oracle_sa_fields(const oracle_solver* s, double* dist, double* nu, double* mut, double* gnu) {
+    if (!s->sa) return;
+    const size_t n = (size_t)s->n, nt = (size_t)s->nt;
+    if (dist) memcpy(dist, s->dist, sizeof(double) * n);
+    if (nu) memcpy(nu, s->nu, sizeof(double) * n);
+    if (mut) memcpy(mut, s->mut, sizeof(double) * nt);
+    if (gnu) memcpy(gnu, s->gnu, sizeof(double) * 3 * nt);
 }

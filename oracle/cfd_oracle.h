@@ -39,6 +39,9 @@ void oracle_jacobian(oracle_solver* s, double cfl, double* alpha, double* values
  * krylov[0]=iterations, krylov[1]=status; returns 0 */
 int oracle_newton_step(oracle_solver* s, double cfl, double* l2, int* krylov);
 int oracle_nvars(const oracle_solver* s);
+/* Spalart-Allmaras fields: wall distance (n), nu_tilde (n), eddy viscosity
+ * (n_total), nu_tilde gradient (3 x n_total); no-op without the model. */
+void oracle_sa_fields(const oracle_solver* s, double* dist, double* nu, double* mut, double* gnu);
 
 /* linear algebra on raw BSR arrays */
 void oracle_bsr_spmv(int n, int bs, const int32_t* rp, const int32_t* cols, const double* vals, const double* x,

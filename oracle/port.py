@@ -40,6 +40,9 @@ def _lib():
         L.oracle_stages.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         L.oracle_jacobian.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
         L.oracle_newton_step.argtypes = [C.c_void_p, C.c_double, _dp, C.POINTER(C.c_int)]
+        L.oracle_nvars.argtypes = [C.c_void_p]
+        L.oracle_nvars.restype = C.c_int
+        L.oracle_sa_fields.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.oracle_bsr_spmv.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_double, C.c_double]
         L.oracle_sgs_apply.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_int]
         L.oracle_bicgstab.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, C.c_int, C.c_double, C.c_double, C.c_int,
@@ -73,6 +76,7 @@ class PortSolver:
         _lib().oracle_create(C.byref(mesh.view), C.byref(cfg), arr, len(bcs), C.byref(h))
         self._h = h
         self.nnzb = int(_lib().oracle_nnzb(self._h))
+        self.nv = int(_lib().oracle_nvars(self._h))
         self.mesh = mesh  # the oracle keeps pointers into the mesh arrays
 
     def close(self):
@@ -93,23 +97,34 @@ class PortSolver:
         return rp, cols
 
     def set_state(self, U):
-        U = np.ascontiguousarray(U, dtype=np.float64).reshape(5, -1)
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.nv, -1)
         _lib().oracle_set_state(self._h, _d(U), U.shape[1])
 
     def get_state(self):
-        U = np.zeros((5, self.n))
+        U = np.zeros((self.nv, self.n))
         _lib().oracle_get_state(self._h, _d(U), self.n)
         return U
 
     def stages(self):
-        n, nt = self.n, self.nt
-        q, grad, phi, res, lam = np.zeros(5 * nt), np.zeros(15 * nt), np.zeros(5 * n), np.zeros(5 * n), np.zeros(n)
+        n, nt, nv = self.n, self.nt, self.nv
+        q, grad, phi, res, lam = np.zeros(5 * nt), np.zeros(15 * nt), np.zeros(5 * n), np.zeros(nv * n), np.zeros(n)
         _lib().oracle_stages(self._h, _d(q), _d(grad), _d(phi), _d(res), _d(lam))
-        return {"q": q, "grad": grad, "phi": phi, "res": res, "lam": lam}
+        out = {"q": q, "grad": grad, "phi": phi, "res": res, "lam": lam}
+        if nv == 6:
+            out.update(self.sa_fields())
+        return out
+
+    def sa_fields(self):
+        """Spalart-Allmaras fields after the last residual: wall distance (n),
+        nu_tilde (n), eddy viscosity (n_total), nu_tilde gradient (3 x n_total)."""
+        n, nt = self.n, self.nt
+        dist, nu, mut, gnu = np.zeros(n), np.zeros(n), np.zeros(nt), np.zeros(3 * nt)
+        _lib().oracle_sa_fields(self._h, _d(dist), _d(nu), _d(mut), _d(gnu))
+        return {"wall_dist": dist, "nu": nu, "mut": mut, "nu_grad": gnu}
 
     def jacobian(self, cfl):
         alpha = np.zeros(self.n)
-        vals = np.zeros(self.nnzb * 25)
+        vals = np.zeros(self.nnzb * self.nv * self.nv)
         _lib().oracle_jacobian(self._h, cfl, _d(alpha), _d(vals))
         return alpha, vals
 
@@ -118,7 +133,7 @@ class PortSolver:
         kr = (C.c_int * 2)()
         _lib().oracle_newton_step(self._h, cfl, _d(l2), kr)
         self.last_krylov = (kr[0], kr[1])
-        return l2[:5]
+        return l2[:self.nv]
 
 
 def bsr_spmv(row_ptr, cols, vals, bs, x, y=None, alpha=1.0, beta=0.0):

@@ -383,6 +383,21 @@ REFH_API int64_t refh_connectivity(const cfdg_mesh_host* m, int kind, int32_t* o
     return static_cast<int64_t>(v.size());
 }
 
+// Reference wall distance (MeshAuxGeometry::add_wall_distance,
+// src/mesh/aux_geometry.cpp:609-696) over the face-neighbour stencil;
+// wall[p] != 0 marks patch p as a wall.
+REFH_API int refh_wall_distance(const cfdg_mesh_host* m, const uint8_t* wall, int n_patches, int max_sweeps,
+                                double rel_tol, double* out) {
+    mesh::MeshPart mp = build_meshpart(*m, true);
+    mesh::MeshAuxConnectivity ac;
+    mesh::MeshAuxGeometry ag;
+    std::vector<bool> wp(static_cast<std::size_t>(n_patches));
+    for (int p = 0; p < n_patches; ++p) wp[p] = wall[p] != 0;
+    ag.add_wall_distance(mp, ac, MPI_COMM_WORLD, wp, mesh::WallDistStencil::FaceNeighbors, max_sweeps, rel_tol);
+    std::copy(ag.cell_wall_dist.begin(), ag.cell_wall_dist.begin() + mp.n_cells, out);
+    return 0;
+}
+
 REFH_API int refh_create(const cfdg_mesh_host* m, const cfdg_config* c, const cfdg_bc_desc* bcs, int nbc,
                          refh_solver** out) {
     mesh::MeshPart mp = build_meshpart(*m, true);

@@ -34,6 +34,7 @@ def _lib():
         L.refh_validate.argtypes = [C.c_void_p]
         L.refh_connectivity.argtypes = [C.c_void_p, C.c_int, _ip, _ip, C.c_int64]
         L.refh_connectivity.restype = C.c_int64
+        L.refh_wall_distance.argtypes = [C.c_void_p, C.POINTER(C.c_uint8), C.c_int, C.c_int, C.c_double, _dp]
         L.refh_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]
         L.refh_destroy.argtypes = [C.c_void_p]
         L.refh_nnzb.argtypes = [C.c_void_p]
@@ -79,6 +80,19 @@ def connectivity(mesh, kind: int):
     val = np.zeros(max(cnt, 1), dtype=np.int32)
     _lib().refh_connectivity(C.byref(mesh.view), kind, _i(off), _i(val), cnt)
     return off, val[:cnt]
+
+
+def wall_distance(mesh, wall_patches, max_sweeps=100000, rel_tol=0.0):
+    """Reference graph wall distance (face-neighbour stencil) to the patches in
+    `wall_patches`; the defaults relax to the exact fixed point."""
+    npatch = int(mesh.view.n_patches)
+    mask = np.zeros(max(npatch, 1), dtype=np.uint8)
+    for p in wall_patches:
+        mask[p] = 1
+    out = np.zeros(mesh.n_cells)
+    _lib().refh_wall_distance(C.byref(mesh.view), mask.ctypes.data_as(C.POINTER(C.c_uint8)), npatch, max_sweeps,
+                              rel_tol, _d(out))
+    return out
 
 
 class RefSolver:
