@@ -44,6 +44,7 @@ PC_NONE, PC_SGS = 0, 1
 KRYLOV_CONVERGED, KRYLOV_DIVERGED, KRYLOV_MAX_ITERATIONS = 0, 1, 2
 (FIELD_U, FIELD_Q, FIELD_GRAD, FIELD_PHI, FIELD_RES, FIELD_LAM, FIELD_DT, FIELD_ALPHA, FIELD_JAC, FIELD_DU,
  FIELD_MUT, FIELD_WALLDIST, FIELD_RHS, FIELD_NU, FIELD_NU_GRAD) = range(15)
+JAC_REFERENCE, JAC_THIN_LAYER = 0, 1
 STAGE_PRIMITIVES, STAGE_GRADIENT, STAGE_LIMITER, STAGE_FLUXES = range(4)
 KCAT_NAMES = ("primitives", "gradient", "limiter", "face_flux", "cell_gather", "jacobian", "lu", "spmv", "sgs",
               "krylov", "update", "turbulence")
@@ -77,7 +78,8 @@ class Config(C.Structure):
                 ("reconstruction", C.c_int32), ("limiter", C.c_int32), ("precision", C.c_int32),
                 ("precond", C.c_int32), ("sgs_ordering", C.c_int32), ("sgs_sweeps", C.c_int32),
                 ("lin_max_iterations", C.c_int32), ("cfl_ramp_iterations", C.c_int32),
-                ("residual_interval", C.c_int32), ("convergence_monitor", C.c_int32), ("reserved_", C.c_int32),
+                ("residual_interval", C.c_int32), ("convergence_monitor", C.c_int32), ("jacobian", C.c_int32),
+                ("limiter_freeze", C.c_int32), ("reserved_", C.c_int32),
                 ("gamma", C.c_double), ("gas_constant", C.c_double), ("prandtl", C.c_double),
                 ("prandtl_turb", C.c_double), ("init_rho", C.c_double), ("init_p", C.c_double),
                 ("init_velocity", C.c_double * 3), ("venkat_k", C.c_double), ("cfl", C.c_double),
@@ -146,6 +148,7 @@ _SIGS = {
     "cfdg_newton_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(StepResult)]),
     "cfdg_residual_norms": (C.c_int, [C.c_void_p, _dp]),
     "cfdg_run_steady": (C.c_int, [C.c_void_p, C.POINTER(RunResult)]),
+    "cfdg_solver_freeze_limiter": (C.c_int, [C.c_void_p, C.c_int32]),
     "cfdg_residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, _dp]),
     "cfdg_solver_stream": (C.c_void_p, [C.c_void_p]),
     "cfdg_solver_launch_count": (C.c_int64, [C.c_void_p]),
@@ -374,6 +377,9 @@ class Solver:
         out = np.zeros(6)
         check(lib().cfdg_residual_norms(self._h, _dptr(out)))
         return out[: self.nvars]
+
+    def freeze_limiter(self, frozen: bool = True):
+        check(lib().cfdg_solver_freeze_limiter(self._h, 1 if frozen else 0))
 
     def run_steady(self) -> RunResult:
         r = RunResult()

@@ -20,7 +20,8 @@ import math
 from dataclasses import dataclass, field
 
 from . import (BC_FARFIELD, BC_NO_SLIP_WALL_HEAT_FLUX, BC_SLIP_WALL, BC_SUBSONIC_INLET, BC_SUBSONIC_OUTLET,
-               BC_SUPERSONIC_INLET, BC_SUPERSONIC_OUTLET, BC_SYMMETRY, GRAD_LSQ_NODE, LIM_VENKATAKRISHNAN,
+               BC_SUPERSONIC_INLET, BC_SUPERSONIC_OUTLET, BC_SYMMETRY, GRAD_LSQ_NODE, JAC_THIN_LAYER,
+               LIM_VENKATAKRISHNAN,
                PC_SGS, PREC_FP64, RECON_MUSCL, SGS_COLOR, MeshSpec, bc, default_config)
 
 GAMMA = 1.4
@@ -77,8 +78,11 @@ def ramp(scale: int = 1, seed: int = 1234, iterations: int = 200) -> Case:
                 {"mach": M, "T": T, "p": p})
 
 
-def plate(scale: int = 1, seed: int = 4321, iterations: int = 200, mixed: bool = False) -> Case:
-    """Laminar flat plate, M=0.5, Re_L=1e5 (256x128x32 hex, 1,048,576 cells)."""
+def plate(scale: int = 1, seed: int = 4321, iterations: int = 200, mixed: bool = False,
+          jacobian: int = JAC_THIN_LAYER) -> Case:
+    """Laminar flat plate, M=0.5, Re_L=1e5 (256x128x32 hex, 1,048,576 cells).
+    `jacobian=JAC_REFERENCE` selects the reference's viscous Jacobian (for
+    comparisons with the reference build)."""
     nx, ny, nz = max(256 // scale, 8), max(128 // scale, 8), max(32 // scale, 2)
     T, M, Re, L = 288.15, 0.5, 1.0e5, 1.0
     u = M * sound_speed(T)
@@ -90,7 +94,7 @@ def plate(scale: int = 1, seed: int = 4321, iterations: int = 200, mixed: bool =
                  jitter=0.10, plate_x0=0.25 * L)
     cfg = default_config(viscous=1, gradient=GRAD_LSQ_NODE, reconstruction=RECON_MUSCL, limiter=LIM_VENKATAKRISHNAN,
                          venkat_k=0.5, precond=PC_SGS, sgs_ordering=SGS_COLOR,
-                         precision=PREC_FP64 if not mixed else 1, prandtl=0.72,
+                         precision=PREC_FP64 if not mixed else 1, prandtl=0.72, jacobian=jacobian,
                          lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
                          cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))
@@ -118,6 +122,7 @@ def sa_plate(scale: int = 1, seed: int = 2468, iterations: int = 200, mixed: boo
     cfg = default_config(viscous=1, turbulence=1, nu_inf_ratio=3.0, gradient=GRAD_LSQ_NODE,
                          reconstruction=RECON_MUSCL, limiter=LIM_VENKATAKRISHNAN, venkat_k=0.5, precond=PC_SGS,
                          sgs_ordering=SGS_COLOR, precision=1 if mixed else PREC_FP64, prandtl=0.72,
+                         jacobian=JAC_THIN_LAYER,
                          lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
                          cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))

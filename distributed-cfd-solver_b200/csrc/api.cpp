@@ -248,6 +248,10 @@ int cfdg_newton_step(cfdg_solver* s, double cfl, cfdg_step_result* out_h) {
     });
 }
 
+int cfdg_solver_freeze_limiter(cfdg_solver* s, int32_t frozen) {
+    CFDG_SOLVER_CALL(s, { s->impl->freeze_limiter(frozen != 0); });
+}
+
 int cfdg_residual_norms(cfdg_solver* s, double* l2_h) {
     if (!l2_h) return CFDG_ERR_INVALID;
     CFDG_SOLVER_CALL(s, s->impl->residual_norms(l2_h));

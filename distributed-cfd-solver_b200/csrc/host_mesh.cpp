@@ -620,25 +620,56 @@ int generate_mesh(const cfdg_mesh_spec& s, HostMesh& m, std::string& err) {
                 m.node_y[n] = y;
                 m.node_z[n] = zs[k];
             }
-    // 2. Seeded jitter of interior nodes, a fraction of the local spacing.
+    // 2. Seeded node jitter, a fraction of the local spacing.
+    //    Plate (wall-normal stretching): every wall-normal grid line moves as
+    //    a whole in x and z (by up to `jitter` of the x / z spacing, wall and
+    //    top nodes included, which stay on their planes) and every row of
+    //    nodes moves as a whole in y (by up to `jitter` of its y spacing).
+    //    The cells stay boxes of random size: a cell 1e-5 high whose top
+    //    and bottom faces were tilted independently would have its centroid
+    //    shifted sideways by ~1e-4, many times its height, and the
+    //    least-squares gradients of the stacked cells would mix the
+    //    wall-normal derivative into the streamwise one.  Other meshes: each
+    //    interior node moves in every coordinate by up to `jitter` of its
+    //    shortest edge.
     if (s.jitter > 0) {
         Rng rng(s.seed ^ 0x9e3779b97f4a7c15ULL);
         std::vector<double> x0(m.node_x), y0(m.node_y), z0(m.node_z);
-        for (int64_t k = 1; k < NZ - 1; ++k)
-            for (int64_t j = 1; j < NY - 1; ++j)
+        auto dist = [&](int32_t a, int32_t b) {
+            const double dx = x0[a] - x0[b], dy = y0[a] - y0[b], dz = z0[a] - z0[b];
+            return std::sqrt(dx * dx + dy * dy + dz * dz);
+        };
+        if (s.kind == 1) {
+            for (int64_t k = 1; k < NZ - 1; ++k)
                 for (int64_t i = 1; i < NX - 1; ++i) {
-                    const int32_t n = nid(i, j, k);
-                    auto dist = [&](int32_t a, int32_t b) {
-                        const double dx = x0[a] - x0[b], dy = y0[a] - y0[b], dz = z0[a] - z0[b];
-                        return std::sqrt(dx * dx + dy * dy + dz * dz);
-                    };
-                    const double hx = std::min(dist(n, nid(i + 1, j, k)), dist(n, nid(i - 1, j, k)));
-                    const double hy = std::min(dist(n, nid(i, j + 1, k)), dist(n, nid(i, j - 1, k)));
-                    const double hz = std::min(dist(n, nid(i, j, k + 1)), dist(n, nid(i, j, k - 1)));
-                    m.node_x[n] = x0[n] + s.jitter * hx * rng.sym();
-                    m.node_y[n] = y0[n] + s.jitter * hy * rng.sym();
-                    m.node_z[n] = z0[n] + s.jitter * hz * rng.sym();
+                    const double hx = std::min(xs[i + 1] - xs[i], xs[i] - xs[i - 1]);
+                    const double hz = std::min(zs[k + 1] - zs[k], zs[k] - zs[k - 1]);
+                    const double ox = s.jitter * hx * rng.sym(), oz = s.jitter * hz * rng.sym();
+                    for (int64_t j = 0; j < NY; ++j) {
+                        const int32_t n = nid(i, j, k);
+                        m.node_x[n] = x0[n] + ox;
+                        m.node_z[n] = z0[n] + oz;
+                    }
                 }
+            for (int64_t j = 1; j < NY - 1; ++j) {
+                const double oy = s.jitter * std::min(ys[j + 1] - ys[j], ys[j] - ys[j - 1]) * rng.sym();
+                for (int64_t k = 0; k < NZ; ++k)
+                    for (int64_t i = 0; i < NX; ++i) m.node_y[nid(i, j, k)] = y0[nid(i, j, k)] + oy;
+            }
+        } else {
+            for (int64_t k = 1; k < NZ - 1; ++k)
+                for (int64_t j = 1; j < NY - 1; ++j)
+                    for (int64_t i = 1; i < NX - 1; ++i) {
+                        const int32_t n = nid(i, j, k);
+                        const double hx = std::min(dist(n, nid(i + 1, j, k)), dist(n, nid(i - 1, j, k)));
+                        const double hy = std::min(dist(n, nid(i, j + 1, k)), dist(n, nid(i, j - 1, k)));
+                        const double hz = std::min(dist(n, nid(i, j, k + 1)), dist(n, nid(i, j, k - 1)));
+                        const double h = std::min(hx, std::min(hy, hz));
+                        m.node_x[n] = x0[n] + s.jitter * h * rng.sym();
+                        m.node_y[n] = y0[n] + s.jitter * h * rng.sym();
+                        m.node_z[n] = z0[n] + s.jitter * h * rng.sym();
+                    }
+        }
     }
     // 3. Cells in CGNS order.
     m.cell_type.clear();

@@ -67,6 +67,7 @@ struct JacStructure {
     const int32_t* diag;      // n
     const int32_t* trans;     // nnzb: position of the transposed block
     const int32_t* face_pos;  // 2*ni: block (owner,neigh), block (neigh,owner)
+    bool full_viscous;        // thin-layer operator with the normal-stress term + no-slip ghost
 };
 template <typename MT>
 void launch_jacobian(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,

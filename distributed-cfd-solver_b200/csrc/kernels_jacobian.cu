@@ -8,6 +8,7 @@
 // its faces, which are minus the transposed off-diagonal blocks, plus the
 // boundary-face blocks and alpha*I; the diagonal kernel gathers them in the
 // same order as the sequential reference adds them.
+#include "cfdg.h"
 #include "kernels.hpp"
 #include "physics.cuh"
 
@@ -47,7 +48,7 @@ __device__ __forceinline__ void warp_store_blocks(MT (*stage)[BS * BS], int32_t 
     __syncwarp();
 }
 
-template <typename MT, bool VISC, int BS>
+template <typename MT, bool VISC, int BS, bool FULL>
 __global__ void __launch_bounds__(128) k_jac_offdiag(DevMesh m, DevFields f, GasParams g, JacStructure js, MT* vals) {
     __shared__ MT stage_all[4][32][BS * BS];
     MT(*stage)[BS * BS] = stage_all[threadIdx.x >> 5];
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(128) k_jac_offdiag(DevMesh m, DevFields f, Gas
     double J[25];
     // A(c0, c1) += dF/dUR
     side_jacobian(g, UR, nx, ny, nz, half_area, -diss, J);
-    if (VISC) viscous_jacobian_add(g, m.finv_d[fcs], qL, qR, mutL, mutR, A, -1.0, J);
+    if (VISC) viscous_jacobian_add<FULL>(g, m.finv_d[fcs], qL, qR, mutL, mutR, A, -1.0, J, nx, ny, nz);
 #pragma unroll
     for (int r = 0; r < BS; ++r)
 #pragma unroll
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(128) k_jac_offdiag(DevMesh m, DevFields f, Gas
     warp_store_blocks<MT, BS>(stage, js.face_pos[2 * fcs], valid, vals);
     // A(c1, c0) -= dF/dUL
     side_jacobian(g, UL, nx, ny, nz, half_area, diss, J);
-    if (VISC) viscous_jacobian_add(g, m.finv_d[fcs], qL, qR, mutL, mutR, A, 1.0, J);
+    if (VISC) viscous_jacobian_add<FULL>(g, m.finv_d[fcs], qL, qR, mutL, mutR, A, 1.0, J, nx, ny, nz);
 #pragma unroll
     for (int r = 0; r < BS; ++r)
 #pragma unroll
@@ -93,8 +94,10 @@ __global__ void __launch_bounds__(128) k_jac_offdiag(DevMesh m, DevFields f, Gas
 }
 
 // Boundary faces: owner-side block only, first-order states against the BC
-// ghost, ghost eddy viscosity zero (jacobian_kernel.hpp:232-269).
-template <bool VISC>
+// ghost, ghost eddy viscosity zero (jacobian_kernel.hpp:232-269).  FULL:
+// the no-slip ghost's mirrored velocity (and isothermal temperature) doubles
+// the owner's viscous derivative.
+template <bool VISC, bool FULL>
 __global__ void __launch_bounds__(128) k_jac_bface(DevMesh m, DevFields f, GasParams g, double* __restrict__ out) {
     const int32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.nb) return;
@@ -116,7 +119,10 @@ __global__ void __launch_bounds__(128) k_jac_bface(DevMesh m, DevFields f, GasPa
     side_jacobian(g, UL, nx, ny, nz, 0.5 * A, 0.5 * smax * A, J);
     if (VISC) {
         const double mutL = f.mut ? f.mut[c0] : 0.0;
-        viscous_jacobian_add(g, m.finv_d[fc], qL, qR, mutL, 0.0, A, 1.0, J);
+        const int kind = m.patches[m.bpatch[b]].kind;
+        const bool noslip = kind == CFDG_BC_NO_SLIP_WALL || kind == CFDG_BC_NO_SLIP_WALL_HEAT_FLUX;
+        const double wv = noslip ? 2.0 : 1.0, wt = kind == CFDG_BC_NO_SLIP_WALL ? 2.0 : 1.0;
+        viscous_jacobian_add<FULL>(g, m.finv_d[fc], qL, qR, mutL, 0.0, A, 1.0, J, nx, ny, nz, wv, wt);
     }
 #pragma unroll
     for (int i = 0; i < 25; ++i) out[int64_t(b) * 25 + i] = J[i];
@@ -150,27 +156,34 @@ __global__ void __launch_bounds__(256) k_jac_diag(DevMesh m, const double* __res
 
 }  // namespace
 
-template <typename MT>
-void launch_jacobian(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,
-                     bool visc, MT* values, double* bface_scratch, cudaStream_t s) {
+template <typename MT, bool FULL>
+static void launch_jacobian_t(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,
+                              bool visc, MT* values, double* bface_scratch, cudaStream_t s) {
     if (m.ni > 0) {
         const unsigned gr = grid_for(m.ni, 128);
         if (bs == 5) {
-            if (visc) k_jac_offdiag<MT, true, 5><<<gr, 128, 0, s>>>(m, f, g, js, values);
-            else k_jac_offdiag<MT, false, 5><<<gr, 128, 0, s>>>(m, f, g, js, values);
+            if (visc) k_jac_offdiag<MT, true, 5, FULL><<<gr, 128, 0, s>>>(m, f, g, js, values);
+            else k_jac_offdiag<MT, false, 5, FULL><<<gr, 128, 0, s>>>(m, f, g, js, values);
         } else {
-            if (visc) k_jac_offdiag<MT, true, 6><<<gr, 128, 0, s>>>(m, f, g, js, values);
-            else k_jac_offdiag<MT, false, 6><<<gr, 128, 0, s>>>(m, f, g, js, values);
+            if (visc) k_jac_offdiag<MT, true, 6, FULL><<<gr, 128, 0, s>>>(m, f, g, js, values);
+            else k_jac_offdiag<MT, false, 6, FULL><<<gr, 128, 0, s>>>(m, f, g, js, values);
         }
     }
     if (m.nb > 0) {
         const unsigned gr = grid_for(m.nb, 128);
-        if (visc) k_jac_bface<true><<<gr, 128, 0, s>>>(m, f, g, bface_scratch);
-        else k_jac_bface<false><<<gr, 128, 0, s>>>(m, f, g, bface_scratch);
+        if (visc) k_jac_bface<true, FULL><<<gr, 128, 0, s>>>(m, f, g, bface_scratch);
+        else k_jac_bface<false, FULL><<<gr, 128, 0, s>>>(m, f, g, bface_scratch);
     }
     const unsigned gd = grid_for(int64_t(m.n) * 25, 256);
     if (bs == 5) k_jac_diag<MT, 5><<<gd, 256, 0, s>>>(m, f.alpha, js, bface_scratch, values);
     else k_jac_diag<MT, 6><<<gd, 256, 0, s>>>(m, f.alpha, js, bface_scratch, values);
+}
+
+template <typename MT>
+void launch_jacobian(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,
+                     bool visc, MT* values, double* bface_scratch, cudaStream_t s) {
+    if (js.full_viscous && visc) launch_jacobian_t<MT, true>(m, f, g, js, bs, visc, values, bface_scratch, s);
+    else launch_jacobian_t<MT, false>(m, f, g, js, bs, visc, values, bface_scratch, s);
 }
 
 template void launch_jacobian<double>(const DevMesh&, const DevFields&, const GasParams&, const JacStructure&, int,

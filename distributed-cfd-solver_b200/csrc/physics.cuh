@@ -250,9 +250,18 @@ __device__ __forceinline__ double viscous_flux(const GasParams& g, const ViscGeo
 
 // ViscousFlux::face_flux_jacobian, thin-layer dFv/dUL (dFv/dUR = -dFv/dUL)
 // (fluxes/viscous.hpp:280-360).  Accumulates into J with factor s.
+//
+// FULL adds the normal-stress term of the thin-layer operator,
+// d tau / d u = mu/d (I + n n^T / 3), which the reference drops (so the
+// normal momentum sees 3/4 of its viscous stiffness).  wv and wt scale the
+// velocity and temperature derivatives: 2 on a no-slip wall face whose
+// ghost mirrors the velocity (u_g = 2 u_w - u) or the temperature
+// (isothermal, T_g = 2 T_w - T), 1 elsewhere.
+template <bool FULL>
 __device__ __forceinline__ void viscous_jacobian_add(const GasParams& g, double inv_d, const double qL[5],
                                                      const double qR[5], double mutL, double mutR, double area,
-                                                     double s, double J[25]) {
+                                                     double s, double J[25], double nx = 0.0, double ny = 0.0,
+                                                     double nz = 0.0, double wv = 1.0, double wt = 1.0) {
     const double p_f = 0.5 * (qL[0] + qR[0]);
     const double u_f = 0.5 * (qL[1] + qR[1]);
     const double v_f = 0.5 * (qL[2] + qR[2]);
@@ -270,17 +279,38 @@ __device__ __forceinline__ void viscous_jacobian_add(const GasParams& g, double 
     const double C_mu = mu_eff * inv_d * area;
     const double C_lam = k_eff * inv_d * area;
     const double V2 = u_f * u_f + v_f * v_f + w_f * w_f;
-    J[5] += s * (-C_mu * u_f * inv_rho);
-    J[6] += s * (C_mu * inv_rho);
-    J[10] += s * (-C_mu * v_f * inv_rho);
-    J[12] += s * (C_mu * inv_rho);
-    J[15] += s * (-C_mu * w_f * inv_rho);
-    J[18] += s * (C_mu * inv_rho);
-    J[20] += s * (C_lam * (0.5 * V2 - cv * T_f) * inv_rho_cv - C_mu * V2 * inv_rho);
-    J[21] += s * (-C_lam * u_f * inv_rho_cv + C_mu * u_f * inv_rho);
-    J[22] += s * (-C_lam * v_f * inv_rho_cv + C_mu * v_f * inv_rho);
-    J[23] += s * (-C_lam * w_f * inv_rho_cv + C_mu * w_f * inv_rho);
-    J[24] += s * (C_lam * inv_rho_cv);
+    if (!FULL) {
+        J[5] += s * (-C_mu * u_f * inv_rho);
+        J[6] += s * (C_mu * inv_rho);
+        J[10] += s * (-C_mu * v_f * inv_rho);
+        J[12] += s * (C_mu * inv_rho);
+        J[15] += s * (-C_mu * w_f * inv_rho);
+        J[18] += s * (C_mu * inv_rho);
+        J[20] += s * (C_lam * (0.5 * V2 - cv * T_f) * inv_rho_cv - C_mu * V2 * inv_rho);
+        J[21] += s * (-C_lam * u_f * inv_rho_cv + C_mu * u_f * inv_rho);
+        J[22] += s * (-C_lam * v_f * inv_rho_cv + C_mu * v_f * inv_rho);
+        J[23] += s * (-C_lam * w_f * inv_rho_cv + C_mu * w_f * inv_rho);
+        J[24] += s * (C_lam * inv_rho_cv);
+    } else {
+        const double n[3] = {nx, ny, nz}, u[3] = {u_f, v_f, w_f};
+        const double un3 = (nx * u_f + ny * v_f + nz * w_f) * (1.0 / 3.0);
+        const double cm = wv * C_mu, cl = wt * C_lam;
+        double Mu[3];  // (I + n n^T / 3) u
+#pragma unroll
+        for (int a = 0; a < 3; ++a) Mu[a] = u[a] + n[a] * un3;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            J[(1 + a) * 5] += s * (-cm * Mu[a] * inv_rho);
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+                J[(1 + a) * 5 + 1 + b] += s * (cm * ((a == b ? 1.0 : 0.0) + n[a] * n[b] * (1.0 / 3.0)) * inv_rho);
+        }
+        const double uMu = u_f * Mu[0] + v_f * Mu[1] + w_f * Mu[2];
+        J[20] += s * (cl * (0.5 * V2 - cv * T_f) * inv_rho_cv - cm * uMu * inv_rho);
+#pragma unroll
+        for (int b = 0; b < 3; ++b) J[21 + b] += s * (-cl * u[b] * inv_rho_cv + cm * Mu[b] * inv_rho);
+        J[24] += s * (cl * inv_rho_cv);
+    }
 }
 
 // ------------------------------------------------------------- limiters

@@ -543,6 +543,8 @@ Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, c
     sa_ = cfg.turbulence == 1;
     if (sa_ && !cfg.viscous) throw Failure{CFDG_ERR_INVALID, "Spalart-Allmaras needs the viscous equations"};
     nv_ = sa_ ? 6 : 5;
+    if (cfg.jacobian != CFDG_JAC_REFERENCE && cfg.jacobian != CFDG_JAC_THIN_LAYER)
+        throw Failure{CFDG_ERR_INVALID, "unknown Jacobian variant"};
     muscl_ = cfg.reconstruction == CFDG_RECON_MUSCL;
     need_grad_ = muscl_ || cfg.viscous;
     if (cfg.gradient != CFDG_GRAD_LSQ_FACE && cfg.gradient != CFDG_GRAD_LSQ_NODE && need_grad_)
@@ -1026,7 +1028,8 @@ void Solver::stage(int st) {
         case CFDG_STAGE_LIMITER:
             if (need_grad_) {
                 ProfScope ps(&prof_, CFDG_KCAT_LIMITER, stream_, 1, ab_.limiter);
-                launch_limiter_ghostgrad(dm_, df_, gas_, muscl_, cfg_.limiter, cfg_.venkat_k, stream_);
+                launch_limiter_ghostgrad(dm_, df_, gas_, muscl_ && !limiter_frozen_, cfg_.limiter, cfg_.venkat_k,
+                                         stream_);
             }
             break;
         case CFDG_STAGE_FLUXES: {
@@ -1071,6 +1074,7 @@ void Solver::assemble_jacobian() {
     js.diag = v.diag;
     js.trans = trans_.p;
     js.face_pos = face_pos_.p;
+    js.full_viscous = cfg_.jacobian == CFDG_JAC_THIN_LAYER;
     {
         ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 3, ab_.jac);
         if (cfg_.precision == CFDG_PREC_MIXED)
@@ -1147,6 +1151,7 @@ cfdg_run_result Solver::run_steady() {
     const bool robust = cfg_.convergence_monitor == 1;
     for (int64_t iter = 1; iter <= cfg_.max_iterations; ++iter) {
         cfdg_step_result st;
+        if (cfg_.limiter_freeze > 0 && iter >= cfg_.limiter_freeze) limiter_frozen_ = true;
         try {
             st = newton_step(cfl_at(iter));
         } catch (const Failure& f) {

@@ -194,6 +194,7 @@ public:
     BsrSystem& system() { return *sys_; }
     void sizes(int64_t* out) const;
     double cfl_at(int64_t iter) const;
+    void freeze_limiter(bool frozen) { limiter_frozen_ = frozen; }
 
 private:
     void setup_mesh(const cfdg_mesh_host& mesh);
@@ -210,6 +211,7 @@ private:
     bool sa_ = false;
     bool need_grad_ = false;
     bool muscl_ = false;
+    bool limiter_frozen_ = false;
     DevMesh dm_{};
     DevFields df_{};
     SaParams sap_{};

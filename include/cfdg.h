@@ -147,6 +147,14 @@ typedef struct cfdg_bc_desc {
     double direction[3];
 } cfdg_bc_desc;
 
+/* Viscous part of the Picard Jacobian.  REFERENCE: the reference's
+ * thin-layer block mu/d * I on the velocity, boundary faces against a frozen
+ * ghost (viscous.hpp:280-360, jacobian_kernel.hpp:232-269).  THIN_LAYER:
+ * mu/d * (I + n n^T / 3) (the normal-stress term) and, on no-slip wall
+ * faces, the ghost's mirrored velocity (isothermal: temperature) doubling
+ * the owner derivative; the residual is the same. */
+enum { CFDG_JAC_REFERENCE = 0, CFDG_JAC_THIN_LAYER = 1 };
+
 /* Solver configuration: SolverConfig + linalg::SolverParams
  * (include/cfd/solver/compressible/config.hpp:94-136, linalg/config.hpp:14-26)
  * plus the CFL ramp, precision, SGS ordering, SA and learned-guess options. */
@@ -169,6 +177,10 @@ typedef struct cfdg_config {
      *    maximum of L2 (robust when a component starts at round-off, e.g.
      *    spanwise momentum of a quasi-2-D case or a uniform initial state). */
     int32_t convergence_monitor;
+    int32_t jacobian;         /* CFDG_JAC_*                                   */
+    /* run_steady freezes the MUSCL limiter values from this iteration on
+     * (0 = never); cfdg_solver_freeze_limiter does it from the host loop */
+    int32_t limiter_freeze;
     int32_t reserved_;
     double gamma, gas_constant, prandtl, prandtl_turb;
     double init_rho, init_p, init_velocity[3];
@@ -265,6 +277,10 @@ CFDG_API int cfdg_assemble_jacobian(cfdg_solver* s);
 CFDG_API int cfdg_linear_solve(cfdg_solver* s, cfdg_krylov_result* out_h);
 /* BackwardEuler::advance (implicit_euler.hpp:34-76) at the given CFL. */
 CFDG_API int cfdg_newton_step(cfdg_solver* s, double cfl, cfdg_step_result* out_h);
+/* Freezes (1) or releases (0) the MUSCL limiter values: while frozen the
+ * residual reuses the last computed phi (a smooth residual for the final
+ * orders of convergence; not in the reference, which recomputes it). */
+CFDG_API int cfdg_solver_freeze_limiter(cfdg_solver* s, int32_t frozen);
 /* Solver::residual_norms (solver.hpp:740-756), nvars doubles. */
 CFDG_API int cfdg_residual_norms(cfdg_solver* s, double* l2_h);
 /* Allocation-free variant of cfdg_residual_norms, with no counterpart in the

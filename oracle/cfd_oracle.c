@@ -275,9 +275,12 @@ static double viscous(const oracle_solver* s, int f, const double* qL, const dou
     return (4.0 / 3.0) * (mu / rho_f) * id * A;
 }
 
-/* ViscousFlux::face_flux_jacobian, thin layer (fluxes/viscous.hpp:280-360). */
+/* ViscousFlux::face_flux_jacobian, thin layer (fluxes/viscous.hpp:280-360).
+ * full != 0 (CFDG_JAC_THIN_LAYER): mu/d (I + n n^T / 3) on the velocity, and
+ * wv / wt scale the velocity / temperature derivatives (2 on a no-slip wall
+ * face for the mirrored ghost velocity / isothermal temperature). */
 static void viscous_jac(const oracle_solver* s, int f, const double* qL, const double* qR, double mutL, double mutR,
-                        double A, double* J) {
+                        double A, double* J, int full, double wv, double wt) {
     const double pf = 0.5 * (qL[0] + qR[0]), uf = 0.5 * (qL[1] + qR[1]), vf = 0.5 * (qL[2] + qR[2]);
     const double wf = 0.5 * (qL[3] + qR[3]), Tf = 0.5 * (qL[4] + qR[4]);
     const double rho = pf / (s->R * Tf), ir = 1.0 / rho, irc = 1.0 / (rho * s->cv);
@@ -286,17 +289,38 @@ static void viscous_jac(const oracle_solver* s, int f, const double* qL, const d
     const double Cm = mu * s->finv_d[f] * A, Cl = k * s->finv_d[f] * A;
     const double V2 = uf * uf + vf * vf + wf * wf;
     memset(J, 0, 25 * sizeof(double));
-    J[5] = -Cm * uf * ir;
-    J[6] = Cm * ir;
-    J[10] = -Cm * vf * ir;
-    J[12] = Cm * ir;
-    J[15] = -Cm * wf * ir;
-    J[18] = Cm * ir;
-    J[20] = Cl * (0.5 * V2 - s->cv * Tf) * irc - Cm * V2 * ir;
-    J[21] = -Cl * uf * irc + Cm * uf * ir;
-    J[22] = -Cl * vf * irc + Cm * vf * ir;
-    J[23] = -Cl * wf * irc + Cm * wf * ir;
-    J[24] = Cl * irc;
+    if (!full) {
+        J[5] = -Cm * uf * ir;
+        J[6] = Cm * ir;
+        J[10] = -Cm * vf * ir;
+        J[12] = Cm * ir;
+        J[15] = -Cm * wf * ir;
+        J[18] = Cm * ir;
+        J[20] = Cl * (0.5 * V2 - s->cv * Tf) * irc - Cm * V2 * ir;
+        J[21] = -Cl * uf * irc + Cm * uf * ir;
+        J[22] = -Cl * vf * irc + Cm * vf * ir;
+        J[23] = -Cl * wf * irc + Cm * wf * ir;
+        J[24] = Cl * irc;
+        return;
+    }
+    const double n[3] = {s->m.face_normal_x[f], s->m.face_normal_y[f], s->m.face_normal_z[f]};
+    const double u[3] = {uf, vf, wf};
+    const double cm = wv * Cm, cl = wt * Cl;
+    double M[3][3], Mu[3] = {0, 0, 0};
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            M[a][b] = (a == b ? 1.0 : 0.0) + n[a] * n[b] / 3.0;
+            Mu[a] += M[a][b] * u[b];
+        }
+    double uMu = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        J[(1 + a) * 5] = -cm * Mu[a] * ir;
+        for (int b = 0; b < 3; ++b) J[(1 + a) * 5 + 1 + b] = cm * M[a][b] * ir;
+        uMu += u[a] * Mu[a];
+    }
+    J[20] = cl * (0.5 * V2 - s->cv * Tf) * irc - cm * uMu * ir;
+    for (int b = 0; b < 3; ++b) J[21 + b] = -cl * u[b] * irc + cm * Mu[b] * ir;
+    J[24] = cl * irc;
 }
 
 /* --------------------------------------------------------------- BCs */
@@ -1158,7 +1182,14 @@ static void jacobian(oracle_solver* s, double cfl) {
         if (s->visc) {
             const double mutL = s->sa ? s->mut[c0] : 0.0;
             const double mutR = (s->sa && inner) ? s->mut[c1] : 0.0;
-            viscous_jac(s, f, qL, qR, mutL, mutR, A, Jv);
+            const int full = s->cfg.jacobian == CFDG_JAC_THIN_LAYER;
+            double wv = 1.0, wt = 1.0;
+            if (full && !inner) {
+                const int kind = s->bcp[m->face_patch[f]].kind;
+                if (kind == CFDG_BC_NO_SLIP_WALL || kind == CFDG_BC_NO_SLIP_WALL_HEAT_FLUX) wv = 2.0;
+                if (kind == CFDG_BC_NO_SLIP_WALL) wt = 2.0;
+            }
+            viscous_jac(s, f, qL, qR, mutL, mutR, A, Jv, full, wv, wt);
             for (int i = 0; i < 25; ++i) {
                 dFL[i] += Jv[i];
                 dFR[i] += -Jv[i];

@@ -24,7 +24,7 @@ import refh  # noqa: E402
 
 CASES = {
     "ramp": lambda cb: cb.cases.ramp(scale=4),
-    "plate": lambda cb: cb.cases.plate(scale=16),
+    "plate": lambda cb: cb.cases.plate(scale=16, jacobian=cb.JAC_REFERENCE),
     "bump": lambda cb: cb.cases.bump(scale=32, mixed=False),
 }
 CFLS = (1.0, 3.0, 10.0)

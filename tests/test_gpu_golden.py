@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
 CASES = {
     "ramp": lambda cb: cb.cases.ramp(scale=4),
-    "plate": lambda cb: cb.cases.plate(scale=16),
+    "plate": lambda cb: cb.cases.plate(scale=16, jacobian=cb.JAC_REFERENCE),
     "bump": lambda cb: cb.cases.bump(scale=32, mixed=False),
 }
 

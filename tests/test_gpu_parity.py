@@ -34,6 +34,7 @@ def _face_stencil(cb, case):
 
 def _setup(cb, refh, name, level=True):
     case = CASES[name](cb)
+    case.cfg.jacobian = cb.JAC_REFERENCE  # the reference's Jacobian
     if level:
         case.cfg.sgs_ordering = cb.SGS_LEVEL
     mesh = cb.HostMesh(case.spec)
@@ -174,3 +175,27 @@ def test_colour_sgs_newton_converges(cb):
         r = s.run_steady()
         assert not r.blowup
         assert r.rel < 2e-2, r.rel
+
+
+def test_thin_layer_jacobian_matches_oracle(cb):
+    """CFDG_JAC_THIN_LAYER (normal-stress term + no-slip ghost) against the
+    oracle restatement of the same variant."""
+    import port
+    case = cb.cases.plate(scale=8, jacobian=cb.JAC_THIN_LAYER)
+    mesh = cb.HostMesh(case.spec)
+    U0 = cb.cases.perturbed_state(case, mesh.n_cells)
+    ora = port.PortSolver(mesh, case.cfg, case.bcs)
+    ora.set_state(U0)
+    ora.stages()
+    _, vals_ref = ora.jacobian(7.5)
+    ref0 = port.PortSolver(mesh, cb.cases.plate(scale=8, jacobian=cb.JAC_REFERENCE).cfg, case.bcs)
+    ref0.set_state(U0)
+    ref0.stages()
+    _, vals0 = ref0.jacobian(7.5)
+    assert rel_err(vals_ref, vals0, 25) > 1e-3  # the variants differ
+    with cb.Solver(mesh, case.cfg, case.bcs) as s:
+        s.set_state(U0)
+        s.evaluate_residual()
+        s.compute_dt(7.5)
+        s.assemble_jacobian()
+        assert rel_err(s.get(cb.FIELD_JAC), vals_ref, 25) < 1e-9

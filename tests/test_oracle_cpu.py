@@ -11,7 +11,7 @@ from conftest import rel_err
 GOLDEN = Path(__file__).resolve().parent / "golden"
 CASES = {
     "ramp": lambda cb: cb.cases.ramp(scale=4),
-    "plate": lambda cb: cb.cases.plate(scale=16),
+    "plate": lambda cb: cb.cases.plate(scale=16, jacobian=cb.JAC_REFERENCE),
     "bump": lambda cb: cb.cases.bump(scale=32, mixed=False),
 }
 
@@ -64,7 +64,7 @@ def test_oracle_matches_golden(cb, port, name):
 
 @pytest.mark.parametrize("name", ["ramp_full", "plate8"])
 def test_oracle_matches_reference_build(cb, refh, port, name):
-    case = cb.cases.ramp() if name == "ramp_full" else cb.cases.plate(scale=8)
+    case = cb.cases.ramp() if name == "ramp_full" else cb.cases.plate(scale=8, jacobian=cb.JAC_REFERENCE)
     case.cfg.sgs_ordering = cb.SGS_LEVEL
     mesh = cb.HostMesh(case.spec)
     U0 = cb.cases.perturbed_state(case, mesh.n_cells, seed=11)

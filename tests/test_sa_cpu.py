@@ -24,8 +24,9 @@ def test_wall_distance_matches_reference(cb, refh, port):
     d_ref = refh.wall_distance(mesh, [3])
     assert np.array_equal(d, d_ref)
     # the reference's default stopping rule (100 sweeps, 1e-4) reaches the
-    # same fixed point on this mesh
-    assert np.array_equal(refh.wall_distance(mesh, [3], 100, 1e-4), d_ref)
+    # same fixed point on this mesh up to the rounding of the path sums
+    d_def = refh.wall_distance(mesh, [3], 100, 1e-4)
+    assert np.all(d_def >= d_ref) and np.allclose(d_def, d_ref, rtol=1e-13, atol=0.0)
     assert d.min() > 0 and d.max() < 2.0
 
 
