@@ -47,10 +47,13 @@ KRYLOV_CONVERGED, KRYLOV_DIVERGED, KRYLOV_MAX_ITERATIONS = 0, 1, 2
 JAC_REFERENCE, JAC_THIN_LAYER = 0, 1
 STAGE_PRIMITIVES, STAGE_GRADIENT, STAGE_LIMITER, STAGE_FLUXES = range(4)
 KCAT_NAMES = ("primitives", "gradient", "limiter", "face_flux", "cell_gather", "jacobian", "lu", "spmv", "sgs",
-              "krylov", "update", "turbulence")
+              "krylov", "update", "turbulence", "guess")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
+_fp = C.POINTER(C.c_float)
+_u16p = C.POINTER(C.c_uint16)
+MLP_IN, MLP_HID, MLP_OUT = 48, 64, 16
 _up = C.POINTER(C.c_uint8)
 
 
@@ -149,6 +152,24 @@ _SIGS = {
     "cfdg_residual_norms": (C.c_int, [C.c_void_p, _dp]),
     "cfdg_run_steady": (C.c_int, [C.c_void_p, C.POINTER(RunResult)]),
     "cfdg_solver_freeze_limiter": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cfdg_tc_selftest": (C.c_int, [C.c_int, C.c_int32, C.c_int32, _u16p, _u16p, _fp]),
+    "cfdg_mlp_create": (C.c_int, [C.c_int, C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "cfdg_mlp_destroy": (C.c_int, [C.c_void_p]),
+    "cfdg_mlp_param_count": (C.c_int32, []),
+    "cfdg_mlp_get_params": (C.c_int, [C.c_void_p, _fp, C.c_int64]),
+    "cfdg_mlp_set_params": (C.c_int, [C.c_void_p, _fp, C.c_int64]),
+    "cfdg_mlp_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+    "cfdg_mlp_forward_host": (C.c_int, [C.c_void_p, _u16p, C.c_int64, _dp]),
+    "cfdg_mlp_gradient_host": (C.c_int, [C.c_void_p, _u16p, _fp, C.c_int64, _fp, _fp]),
+    "cfdg_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _fp]),
+    "cfdg_dataset_create": (C.c_int, [C.c_int, C.c_int32, C.c_int64, C.POINTER(C.c_void_p)]),
+    "cfdg_dataset_destroy": (C.c_int, [C.c_void_p]),
+    "cfdg_dataset_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "cfdg_dataset_clear": (C.c_int, [C.c_void_p]),
+    "cfdg_dataset_append_host": (C.c_int, [C.c_void_p, _u16p, _fp, C.c_int64]),
+    "cfdg_dataset_read_host": (C.c_int, [C.c_void_p, _u16p, _fp, C.c_int64]),
+    "cfdg_solver_attach_guess": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cfdg_solver_attach_dataset": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "cfdg_residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, _dp]),
     "cfdg_solver_stream": (C.c_void_p, [C.c_void_p]),
     "cfdg_solver_launch_count": (C.c_int64, [C.c_void_p]),
@@ -378,6 +399,12 @@ class Solver:
         check(lib().cfdg_residual_norms(self._h, _dptr(out)))
         return out[: self.nvars]
 
+    def attach_guess(self, mlp: "Mlp | None"):
+        check(lib().cfdg_solver_attach_guess(self._h, mlp._h if mlp is not None else None))
+
+    def attach_dataset(self, ds: "Dataset | None", stride: int = 1):
+        check(lib().cfdg_solver_attach_dataset(self._h, ds._h if ds is not None else None, stride))
+
     def freeze_limiter(self, frozen: bool = True):
         check(lib().cfdg_solver_freeze_limiter(self._h, 1 if frozen else 0))
 
@@ -407,6 +434,130 @@ class Solver:
         f, b = C.c_int32(), C.c_int32()
         check(lib().cfdg_solver_sgs_info(self._h, C.byref(f), C.byref(b)))
         return f.value, b.value
+
+
+def _u16(a: np.ndarray):
+    return a.ctypes.data_as(_u16p)
+
+
+def _f32(a: np.ndarray):
+    return a.ctypes.data_as(_fp)
+
+
+def to_bf16_bits(x) -> np.ndarray:
+    """float array -> bf16 bit patterns (round to nearest even)."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return u.astype(np.uint16)
+
+
+def from_bf16_bits(b) -> np.ndarray:
+    return (np.ascontiguousarray(b, dtype=np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+def tc_selftest(a_bits: np.ndarray, b_bits: np.ndarray, device: int = 0) -> np.ndarray:
+    """D[128 x n] = A[128 x k] B[n x k]^T on the tcgen05 tensor cores."""
+    a = np.ascontiguousarray(a_bits, dtype=np.uint16)
+    b = np.ascontiguousarray(b_bits, dtype=np.uint16)
+    n, k = b.shape
+    d = np.zeros((128, n), dtype=np.float32)
+    check(lib().cfdg_tc_selftest(device, n, k, _u16(a), _u16(b), _f32(d)))
+    return d
+
+
+class Mlp:
+    """cfdg_mlp: the learned initial-guess network (device resident)."""
+
+    def __init__(self, nvars: int, seed: int = 1, device: int = 0):
+        h = C.c_void_p()
+        check(lib().cfdg_mlp_create(device, nvars, seed, C.byref(h)))
+        self._h = h
+        self.nvars = nvars
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cfdg_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def param_count() -> int:
+        return int(lib().cfdg_mlp_param_count())
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.param_count(), dtype=np.float32)
+        check(lib().cfdg_mlp_get_params(self._h, _f32(p), p.size))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib().cfdg_mlp_set_params(self._h, _f32(p), p.size))
+
+    def forward(self, feat_bits: np.ndarray) -> np.ndarray:
+        f = np.ascontiguousarray(feat_bits, dtype=np.uint16).reshape(-1, MLP_IN)
+        out = np.zeros((f.shape[0], self.nvars))
+        check(lib().cfdg_mlp_forward_host(self._h, _u16(f), f.shape[0], _dptr(out)))
+        return out
+
+    def gradient(self, feat_bits: np.ndarray, target: np.ndarray):
+        f = np.ascontiguousarray(feat_bits, dtype=np.uint16).reshape(-1, MLP_IN)
+        t = np.ascontiguousarray(target, dtype=np.float32).reshape(-1, MLP_OUT)
+        loss = C.c_float()
+        g = np.zeros(self.param_count(), dtype=np.float32)
+        check(lib().cfdg_mlp_gradient_host(self._h, _u16(f), _f32(t), f.shape[0], C.byref(loss), _f32(g)))
+        return float(loss.value), g
+
+    def train(self, ds: "Dataset", epochs: int = 1, batch: int = 4096, lr: float = 1e-3, seed: int = 7) -> float:
+        loss = C.c_float()
+        check(lib().cfdg_mlp_train(self._h, ds._h, epochs, batch, lr, seed, C.byref(loss)))
+        return float(loss.value)
+
+
+class Dataset:
+    """cfdg_dataset: device buffer of (features, normalised dU) samples."""
+
+    def __init__(self, nvars: int, capacity: int, device: int = 0):
+        h = C.c_void_p()
+        check(lib().cfdg_dataset_create(device, nvars, capacity, C.byref(h)))
+        self._h = h
+        self.nvars = nvars
+        self.capacity = capacity
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cfdg_dataset_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        n = C.c_int64()
+        check(lib().cfdg_dataset_size(self._h, C.byref(n)))
+        return int(n.value)
+
+    def clear(self):
+        check(lib().cfdg_dataset_clear(self._h))
+
+    def append(self, feat_bits, target):
+        f = np.ascontiguousarray(feat_bits, dtype=np.uint16).reshape(-1, MLP_IN)
+        t = np.ascontiguousarray(target, dtype=np.float32).reshape(-1, MLP_OUT)
+        check(lib().cfdg_dataset_append_host(self._h, _u16(f), _f32(t), f.shape[0]))
+
+    def read(self, rows: int | None = None):
+        rows = len(self) if rows is None else rows
+        f = np.zeros((rows, MLP_IN), dtype=np.uint16)
+        t = np.zeros((rows, MLP_OUT), dtype=np.float32)
+        check(lib().cfdg_dataset_read_host(self._h, _u16(f), _f32(t), rows))
+        return f, t
 
 
 class Bsr:

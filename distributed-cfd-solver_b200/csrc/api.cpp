@@ -2,6 +2,7 @@
 // failures into a status code and keeps the message for cfdg_last_error().
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -22,6 +23,15 @@ struct cfdg_bsr {
 };
 struct cfdg_host_mesh {
     cfdg::HostMesh mesh;
+};
+struct cfdg_mlp {
+    cfdg::Mlp* impl;
+    cudaStream_t stream;
+    int device;
+};
+struct cfdg_dataset {
+    cfdg::Dataset* impl;
+    int device;
 };
 
 namespace cfdg {
@@ -415,6 +425,216 @@ int cfdg_bicgstab_host(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_
         x.get(x_h, N, a->stream);
         if (out_h) *out_h = r;
     });
+}
+
+/* ----------------------------------------------------- learned guess */
+int cfdg_tc_selftest(int device, int32_t n, int32_t k, const uint16_t* a_h, const uint16_t* b_h, float* d_h) {
+    if (!a_h || !b_h || !d_h) return CFDG_ERR_INVALID;
+    if (!(n == 16 || n == 32 || n == 48 || n == 64) || k < 16 || k > 128 || k % 16) return CFDG_ERR_INVALID;
+    const int dev = require_device(device);
+    if (dev != CFDG_OK) return dev;
+    return guarded([&] {
+        cfdg::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        uint16_t *A = nullptr, *B = nullptr;
+        float* D = nullptr;
+        int* err = nullptr;
+        auto release = [&] {
+            cudaFree(A);
+            cudaFree(B);
+            cudaFree(D);
+            cudaFree(err);
+        };
+        try {
+            cfdg::cuda_check(cudaMalloc(reinterpret_cast<void**>(&A), 128 * k * 2), "cudaMalloc");
+            cfdg::cuda_check(cudaMalloc(reinterpret_cast<void**>(&B), 64 * k * 2), "cudaMalloc");
+            cfdg::cuda_check(cudaMalloc(reinterpret_cast<void**>(&D), 128 * 64 * 4), "cudaMalloc");
+            cfdg::cuda_check(cudaMalloc(reinterpret_cast<void**>(&err), 4), "cudaMalloc");
+            cfdg::cuda_check(cudaMemset(err, 0, 4), "memset");
+            cfdg::cuda_check(cudaMemcpy(A, a_h, 128 * k * 2, cudaMemcpyHostToDevice), "H2D");
+            cfdg::cuda_check(cudaMemcpy(B, b_h, n * k * 2, cudaMemcpyHostToDevice), "H2D");
+            cfdg::launch_tc_selftest(A, B, D, n, k, err, nullptr);
+            cfdg::cuda_check(cudaGetLastError(), "selftest launch");
+            cfdg::cuda_check(cudaDeviceSynchronize(), "selftest");
+            int e = 0;
+            cfdg::cuda_check(cudaMemcpy(&e, err, 4, cudaMemcpyDeviceToHost), "D2H");
+            if (e) throw cfdg::Failure{CFDG_ERR_CUDA, "tensor-core self-test: MMA completion wait timed out"};
+            cfdg::cuda_check(cudaMemcpy(d_h, D, 128 * n * 4, cudaMemcpyDeviceToHost), "D2H");
+        } catch (...) {
+            release();
+            throw;
+        }
+        release();
+    });
+}
+
+int cfdg_mlp_create(int device, int32_t nvars, uint64_t seed, cfdg_mlp** out) {
+    if (!out) return CFDG_ERR_INVALID;
+    *out = nullptr;
+    const int dev = require_device(device);
+    if (dev != CFDG_OK) return dev;
+    return guarded([&] {
+        cfdg::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        auto* m = new cfdg_mlp{nullptr, nullptr, device};
+        try {
+            cfdg::cuda_check(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            m->impl = new cfdg::Mlp(device, nvars, seed);
+        } catch (...) {
+            if (m->stream) cudaStreamDestroy(m->stream);
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+int cfdg_mlp_destroy(cfdg_mlp* m) {
+    if (!m) return CFDG_OK;
+    const int st = guarded([&] {
+        cudaSetDevice(m->device);
+        delete m->impl;
+        if (m->stream) cudaStreamDestroy(m->stream);
+    });
+    delete m;
+    return st;
+}
+
+#define CFDG_MLP_CALL(m, ...)                        \
+    if (!(m) || !(m)->impl) return CFDG_ERR_INVALID; \
+    return guarded([&] { cudaSetDevice((m)->device); __VA_ARGS__; })
+
+int32_t cfdg_mlp_param_count(void) { return cfdg::kMlpParams; }
+
+int cfdg_mlp_get_params(cfdg_mlp* m, float* out_h, int64_t count) {
+    if (!out_h || count < cfdg::kMlpParams) return CFDG_ERR_INVALID;
+    CFDG_MLP_CALL(m, m->impl->get_params(out_h));
+}
+
+int cfdg_mlp_set_params(cfdg_mlp* m, const float* p_h, int64_t count) {
+    if (!p_h || count < cfdg::kMlpParams) return CFDG_ERR_INVALID;
+    CFDG_MLP_CALL(m, m->impl->set_params(p_h));
+}
+
+int cfdg_mlp_forward(cfdg_mlp* m, const uint16_t* feat_d, int64_t rows, const double* scale_d, double* out_d) {
+    if (!feat_d || !scale_d || !out_d || rows < 0) return CFDG_ERR_INVALID;
+    CFDG_MLP_CALL(m, {
+        m->impl->forward(feat_d, rows, scale_d, out_d, m->stream);
+        cfdg::cuda_check(cudaStreamSynchronize(m->stream), "sync");
+    });
+}
+
+int cfdg_mlp_forward_host(cfdg_mlp* m, const uint16_t* feat_h, int64_t rows, double* out_h) {
+    if (!feat_h || !out_h || rows < 0) return CFDG_ERR_INVALID;
+    CFDG_MLP_CALL(m, {
+        const int nv = m->impl->nvars();
+        uint16_t* F = nullptr;
+        double *O = nullptr, *S = nullptr;
+        auto release = [&] {
+            cudaFree(F);
+            cudaFree(O);
+            cudaFree(S);
+        };
+        try {
+            cfdg::cuda_check(cudaMalloc(reinterpret_cast<void**>(&F), std::max<int64_t>(rows, 1) * cfdg::kMlpIn * 2),
+                             "cudaMalloc");
+            cfdg::cuda_check(cudaMalloc(reinterpret_cast<void**>(&O), std::max<int64_t>(rows, 1) * nv * 8), "cudaMalloc");
+            cfdg::cuda_check(cudaMalloc(reinterpret_cast<void**>(&S), 8 * 8), "cudaMalloc");
+            const double ones[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+            cfdg::cuda_check(cudaMemcpy(S, ones, sizeof(ones), cudaMemcpyHostToDevice), "H2D");
+            cfdg::cuda_check(cudaMemcpy(F, feat_h, rows * cfdg::kMlpIn * 2, cudaMemcpyHostToDevice), "H2D");
+            m->impl->forward(F, rows, S, O, m->stream);
+            cfdg::cuda_check(cudaStreamSynchronize(m->stream), "sync");
+            cfdg::cuda_check(cudaMemcpy(out_h, O, rows * nv * 8, cudaMemcpyDeviceToHost), "D2H");
+        } catch (...) {
+            release();
+            throw;
+        }
+        release();
+    });
+}
+
+int cfdg_mlp_gradient_host(cfdg_mlp* m, const uint16_t* x_h, const float* t_h, int64_t rows, float* loss_h,
+                           float* grad_h) {
+    if (!x_h || !t_h || rows <= 0) return CFDG_ERR_INVALID;
+    CFDG_MLP_CALL(m, {
+        cfdg::Dataset tmp(m->device, m->impl->nvars(), rows);
+        tmp.append_host(x_h, t_h, rows);
+        const float l = m->impl->gradient(tmp.X(), tmp.T(), rows, grad_h, m->stream);
+        if (loss_h) *loss_h = l;
+    });
+}
+
+int cfdg_mlp_train(cfdg_mlp* m, cfdg_dataset* ds, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                   float* loss_h) {
+    if (!ds || !ds->impl || epochs < 1 || !(lr > 0.0f)) return CFDG_ERR_INVALID;
+    CFDG_MLP_CALL(m, {
+        const float l = m->impl->train(*ds->impl, epochs, batch, lr, seed, m->stream);
+        if (loss_h) *loss_h = l;
+    });
+}
+
+int cfdg_dataset_create(int device, int32_t nvars, int64_t capacity, cfdg_dataset** out) {
+    if (!out) return CFDG_ERR_INVALID;
+    *out = nullptr;
+    const int dev = require_device(device);
+    if (dev != CFDG_OK) return dev;
+    return guarded([&] {
+        auto* d = new cfdg_dataset{nullptr, device};
+        try {
+            d->impl = new cfdg::Dataset(device, nvars, capacity);
+        } catch (...) {
+            delete d;
+            throw;
+        }
+        *out = d;
+    });
+}
+
+int cfdg_dataset_destroy(cfdg_dataset* d) {
+    if (!d) return CFDG_OK;
+    const int st = guarded([&] {
+        cudaSetDevice(d->device);
+        delete d->impl;
+    });
+    delete d;
+    return st;
+}
+
+int cfdg_dataset_size(const cfdg_dataset* d, int64_t* size_h) {
+    if (!d || !d->impl || !size_h) return CFDG_ERR_INVALID;
+    *size_h = d->impl->size();
+    return CFDG_OK;
+}
+
+int cfdg_dataset_clear(cfdg_dataset* d) {
+    if (!d || !d->impl) return CFDG_ERR_INVALID;
+    d->impl->clear();
+    return CFDG_OK;
+}
+
+int cfdg_dataset_append_host(cfdg_dataset* d, const uint16_t* x_h, const float* t_h, int64_t rows) {
+    if (!d || !d->impl || !x_h || !t_h || rows < 0) return CFDG_ERR_INVALID;
+    return guarded([&] {
+        cudaSetDevice(d->device);
+        d->impl->append_host(x_h, t_h, rows);
+    });
+}
+
+int cfdg_dataset_read_host(const cfdg_dataset* d, uint16_t* x_h, float* t_h, int64_t rows) {
+    if (!d || !d->impl || rows < 0) return CFDG_ERR_INVALID;
+    return guarded([&] {
+        cudaSetDevice(d->device);
+        d->impl->read_host(x_h, t_h, rows);
+    });
+}
+
+int cfdg_solver_attach_guess(cfdg_solver* s, cfdg_mlp* m) {
+    if (m && !m->impl) return CFDG_ERR_INVALID;
+    CFDG_SOLVER_CALL(s, s->impl->attach_guess(m ? m->impl : nullptr));
+}
+
+int cfdg_solver_attach_dataset(cfdg_solver* s, cfdg_dataset* d, int32_t stride) {
+    if (d && !d->impl) return CFDG_ERR_INVALID;
+    CFDG_SOLVER_CALL(s, s->impl->attach_dataset(d ? d->impl : nullptr, stride));
 }
 
 }  // extern "C"

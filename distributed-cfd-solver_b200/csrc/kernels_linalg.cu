@@ -270,12 +270,18 @@ __device__ __forceinline__ double block_sum_partials(const double* __restrict__ 
 
 __global__ void k_krylov_init_fin(KrylovScalars* ks, const double* __restrict__ partials, int nblocks) {
     const double bnorm = sqrt(block_sum_partials(partials, nblocks, 2, 0));
-    const double rnorm = sqrt(block_sum_partials(partials, nblocks, 2, 1));
+    double rnorm = sqrt(block_sum_partials(partials, nblocks, 2, 1));
     if (threadIdx.x != 0) return;
     const double scale = (bnorm > 0.0) ? bnorm : 1.0;
     ks->bnorm = bnorm;
     ks->scale = scale;
     ks->tol = fmax(ks->abs_tol, ks->rel_tol * scale);
+    double r0n = rnorm;
+    if (ks->guess == 1 && !(rnorm < bnorm)) {  // the guess does not beat x = 0
+        ks->guess = 2;
+        r0n = bnorm;
+    }
+    rnorm = r0n;
     ks->initial = rnorm;
     ks->rnorm = rnorm;
     ks->it = 0;
@@ -497,6 +503,25 @@ void launch_krylov_init(int64_t len, const double* b, const double* v, double* r
     k_krylov_init<<<gr, 256, 0, s>>>(len, b, v, r, r0, p, partials);
     k_krylov_init_fin<<<1, kFinThreads, 0, s>>>(ks, partials, static_cast<int>(gr));
 }
+__global__ void __launch_bounds__(256) k_krylov_guess_reset(int64_t len, const KrylovScalars* __restrict__ ks,
+                                                            const double* __restrict__ b, double* __restrict__ x,
+                                                            double* __restrict__ r, double* __restrict__ r0,
+                                                            double* __restrict__ p) {
+    if (ks->guess != 2) return;  // uniform
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= len) return;
+    const double bt = b[t];
+    x[t] = 0.0;
+    r[t] = bt;
+    r0[t] = bt;
+    p[t] = bt;
+}
+
+void launch_krylov_guess_reset(int64_t len, const KrylovScalars* ks, const double* b, double* x, double* r, double* r0,
+                               double* p, cudaStream_t s) {
+    k_krylov_guess_reset<<<grid_for(len, 256), 256, 0, s>>>(len, ks, b, x, r, r0, p);
+}
+
 void launch_krylov_begin(KrylovScalars* ks, cudaStream_t s) { k_krylov_begin<<<1, 32, 0, s>>>(ks); }
 void launch_krylov_gamma(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s) {
     k_krylov_gamma<<<1, kFinThreads, 0, s>>>(ks, partials, nblocks);

@@ -17,7 +17,7 @@ struct KrylovScalars {
     int state;
     int it;
     int max_it;
-    int pad_;
+    int guess;  // in: 1 when x holds an initial guess that may be rejected; out: 2 when rejected
     double rel_tol, abs_tol;
     double bnorm, scale, tol, initial, rnorm;
     double rho, rho_old, rho_new, alpha, omega, omega_new, beta;
@@ -40,6 +40,10 @@ void launch_dots(int64_t len, const DotSpec& ds, double* partials, cudaStream_t 
 void launch_copy(int64_t len, const double* a, double* b, const int* active, cudaStream_t s);
 void launch_krylov_init(int64_t len, const double* b, const double* v, double* r, double* r0, double* p,
                         double* partials, KrylovScalars* ks, cudaStream_t s);
+// After launch_krylov_init: a rejected initial guess (||b - A x0|| >=
+// ||b||) restarts from x = 0 (r = r0 = p = b).
+void launch_krylov_guess_reset(int64_t len, const KrylovScalars* ks, const double* b, double* x, double* r, double* r0,
+                               double* p, cudaStream_t s);
 void launch_krylov_begin(KrylovScalars* ks, cudaStream_t s);
 void launch_krylov_gamma(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s);
 void launch_krylov_s(int64_t len, const KrylovScalars* ks, const double* r, const double* v, double* sv,

@@ -431,7 +431,7 @@ void BsrSystem::sgs_apply(const double* r, double* z, const int* active) {
 }
 
 cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_tol, int max_it, double* x,
-                                       const double* b) {
+                                       const double* b, bool guess) {
     if (precond == CFDG_PC_SGS && !lu_ready_) throw Failure{CFDG_ERR_INVALID, "SGS preconditioner not set up"};
     const int64_t N = int64_t(n_) * bs_;
     const BsrView A = view();
@@ -440,6 +440,7 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
     init.max_it = max_it;
     init.rel_tol = rel_tol;
     init.abs_tol = abs_tol;
+    init.guess = guess ? 1 : 0;
     cuda_check(cudaMemcpyAsync(ks_.p, &init, sizeof(init), cudaMemcpyHostToDevice, stream_), "H2D");
     const int* active = &ks_.p->state;
     auto spmv_dots = [&](const double* xin, double* yout, const DotSpec& ds) {
@@ -458,6 +459,10 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
         }
         ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 2, 5.0 * 8.0 * N);
         launch_krylov_init(N, b, v_.p, r_.p, r0_.p, p_.p, partials_.p, ks_.p, stream_);
+        if (guess) {
+            ++prof_->launches;
+            launch_krylov_guess_reset(N, ks_.p, b, x, r_.p, r0_.p, p_.p, stream_);
+        }
     }
     const int nblk = spmv_blocks(n_, bs_);
     const int nvec = dot_blocks(N);
@@ -516,6 +521,7 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
     cuda_check(cudaGetLastError(), "krylov launch");
     cuda_check(cudaMemcpyAsync(ks_host_, ks_.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, stream_), "D2H");
     cuda_check(cudaStreamSynchronize(stream_), "krylov sync");
+    last_guess_ = guess ? ks_host_->guess : 0;
     cfdg_krylov_result res{};
     switch (ks_host_->state) {
         case KS_CONVERGED: res.status = CFDG_KRYLOV_CONVERGED; break;
@@ -1094,9 +1100,69 @@ void Solver::assemble_jacobian() {
 
 cfdg_krylov_result Solver::linear_solve() {
     if (cfg_.precond == CFDG_PC_SGS) sys_->sgs_setup(cfg_.sgs_ordering, std::max(cfg_.sgs_sweeps, 1));
-    cuda_check(cudaMemsetAsync(du_.p, 0, du_.count * sizeof(double), stream_), "memset");
-    last_krylov_ = sys_->bicgstab(cfg_.precond, cfg_.lin_rel_tol, cfg_.lin_abs_tol, cfg_.lin_max_iterations, du_.p, b_.p);
+    if (guess_ || dataset_) prepare_guess_inputs();
+    if (guess_) {
+        ProfScope ps(&prof_, CFDG_KCAT_GUESS, stream_, 1, double(dm_.n) * (kMlpIn * 2.0 + nv_ * 8.0));
+        guess_->forward(feat_.p, dm_.n, gscale_.p, du_.p, stream_);
+    } else {
+        cuda_check(cudaMemsetAsync(du_.p, 0, du_.count * sizeof(double), stream_), "memset");
+    }
+    last_krylov_ = sys_->bicgstab(cfg_.precond, cfg_.lin_rel_tol, cfg_.lin_abs_tol, cfg_.lin_max_iterations, du_.p,
+                                  b_.p, guess_ != nullptr);
     return last_krylov_;
+}
+
+void Solver::learn_alloc() {
+    if (feat_.p) return;
+    const std::size_t n = static_cast<std::size_t>(dm_.n);
+    alloc_or_throw(feat_, n * kMlpIn, "guess features");
+    alloc_or_throw(du_prev_, n * nv_, "previous update");
+    alloc_or_throw(gscale_, 32, "guess scales");
+    alloc_or_throw(gpart_, static_cast<std::size_t>(guess_sum_blocks(dm_.n)) * 2 * nv_ + 8, "guess partials");
+    cuda_check(cudaMemsetAsync(du_prev_.p, 0, du_prev_.count * sizeof(double), stream_), "memset");
+    // free-stream scales and state (conserved) for the state features
+    const double rho = cfg_.init_rho, p = cfg_.init_p;
+    const double u = cfg_.init_velocity[0], v = cfg_.init_velocity[1], w = cfg_.init_velocity[2];
+    const double T = p / (rho * gas_.R);
+    const double a = std::sqrt(gas_.gamma * gas_.R * T);
+    const double E = rho * gas_.cv * T + 0.5 * rho * (u * u + v * v + w * w);
+    const double spd = std::max(std::sqrt(u * u + v * v + w * w), a);
+    double h[32] = {};
+    const double su[6] = {rho, rho * spd, rho * spd, rho * spd, E, sa_ ? std::max(rho * sap_.nu_inf, 1e-300) : 1.0};
+    const double ui[6] = {rho, rho * u, rho * v, rho * w, E, sa_ ? rho * sap_.nu_inf : 0.0};
+    for (int k = 0; k < 8; ++k) h[k] = h[8 + k] = 1.0;
+    for (int k = 0; k < 6; ++k) {
+        h[16 + k] = su[k];
+        h[24 + k] = ui[k];
+    }
+    cuda_check(cudaMemcpyAsync(gscale_.p, h, sizeof(h), cudaMemcpyHostToDevice, stream_), "H2D");
+    cuda_check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void Solver::prepare_guess_inputs() {
+    ProfScope ps(&prof_, CFDG_KCAT_GUESS, stream_, 3,
+                 double(dm_.n) * (nv_ * 8.0 * 4 + 16.0) +
+                     double(dm_.n) * (kMlpIn * 2.0 + 8.0 * (nv_ * 3 + 2)) + double(c2c_.count) * 4.0);
+    launch_guess_scales(dm_.n, nv_, b_.p, dt_.p, vol_.p, du_prev_.p, gpart_.p, gscale_.p, stream_);
+    launch_guess_features(dm_, nv_, U_.p, b_.p, dt_.p, du_prev_.p, gscale_.p, feat_.p, stream_);
+    cuda_check(cudaGetLastError(), "guess launch");
+}
+
+void Solver::attach_guess(Mlp* m) {
+    if (m && (m->nvars() != nv_ || m->device() != device_))
+        throw Failure{CFDG_ERR_INVALID, "network variable count or device does not match the solver"};
+    if (m) learn_alloc();
+    guess_ = m;
+}
+
+void Solver::attach_dataset(Dataset* d, int32_t stride) {
+    if (d && (d->nvars() != nv_ || d->device() != device_))
+        throw Failure{CFDG_ERR_INVALID, "dataset variable count or device does not match the solver"};
+    if (d && stride < 1) throw Failure{CFDG_ERR_INVALID, "dataset stride must be >= 1"};
+    if (d) learn_alloc();
+    dataset_ = d;
+    ds_stride_ = std::max(stride, 1);
+    ds_phase_ = 0;
 }
 
 void Solver::residual_norms(double* l2_host) {
@@ -1116,10 +1182,24 @@ cfdg_step_result Solver::newton_step(double cfl) {
     compute_dt(cfl);
     assemble_jacobian();
     const cfdg_krylov_result kr = linear_solve();
+    if (dataset_) {
+        const int64_t want = (int64_t(dm_.n) - ds_phase_ + ds_stride_ - 1) / ds_stride_;
+        const int64_t at = dataset_->size();
+        const int64_t got = dataset_->reserve(want);
+        if (got > 0) {
+            ProfScope ps(&prof_, CFDG_KCAT_GUESS, stream_, 1, double(got) * (kMlpIn * 4.0 + nv_ * 8.0 + kMlpOut * 4.0));
+            launch_guess_append(dm_.n, nv_, ds_stride_, ds_phase_, got, feat_.p, du_.p, gscale_.p,
+                                dataset_->X() + at * kMlpIn, dataset_->T() + at * kMlpOut, stream_);
+        }
+        ds_phase_ = (ds_phase_ + 1) % ds_stride_;
+    }
     {
         ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, ab_.state_update);
         launch_state_update(dm_, U_.p, du_.p, nv_, stream_);
     }
+    if (guess_ || dataset_)
+        cuda_check(cudaMemcpyAsync(du_prev_.p, du_.p, du_.count * sizeof(double), cudaMemcpyDeviceToDevice, stream_),
+                   "D2D");
     residual_norms(r.l2);
     r.cfl = cfl;
     r.nvars = nv_;
@@ -1127,7 +1207,7 @@ cfdg_step_result Solver::newton_step(double cfl) {
     r.krylov_iterations = kr.iterations;
     r.krylov_initial = kr.initial_residual;
     r.krylov_final = kr.final_residual;
-    r.guess_used = 0;
+    r.guess_used = guess_ ? sys_->last_guess() : 0;
     return r;
 }
 

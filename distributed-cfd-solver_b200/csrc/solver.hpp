@@ -14,6 +14,7 @@
 #include "device_common.cuh"
 #include "host_mesh.hpp"
 #include "kernels.hpp"
+#include "guess.hpp"
 #include "krylov.hpp"
 
 namespace cfdg {
@@ -133,7 +134,11 @@ public:
     // z = M^-1 r (device vectors).
     void sgs_apply(const double* r, double* z, const int* active);
     // BiCGSTAB on device vectors; x holds the initial guess.
-    cfdg_krylov_result bicgstab(int precond, double rel_tol, double abs_tol, int max_it, double* x, const double* b);
+    // guess: x holds an initial guess that is replaced by x = 0 when
+    // ||b - A x|| >= ||b||; last_guess() tells 1 accepted, 2 rejected.
+    cfdg_krylov_result bicgstab(int precond, double rel_tol, double abs_tol, int max_it, double* x, const double* b,
+                                bool guess = false);
+    int last_guess() const { return last_guess_; }
     int groups_fwd() const { return static_cast<int>(fwd_off_.size()) - 1; }
     int groups_bwd() const { return static_cast<int>(bwd_off_.size()) - 1; }
     int64_t launches() const { return prof_->launches; }
@@ -158,6 +163,7 @@ private:
     DevArray<int8_t> piv_;
     DevArray<int> err_;
     int ordering_ = -1, sweeps_ = 1;
+    int last_guess_ = 0;
     bool lu_ready_ = false;
     std::vector<int32_t> fwd_off_, bwd_off_;
     std::vector<double> fwd_bytes_[2], bwd_bytes_[2];  // algorithmic bytes of one pass, mode 0 / mode 1
@@ -194,6 +200,10 @@ public:
     BsrSystem& system() { return *sys_; }
     void sizes(int64_t* out) const;
     double cfl_at(int64_t iter) const;
+    // learned initial guess of the linear solve (nullptr: zero guess) and
+    // the dataset that receives (features, dU) of every stride-th cell
+    void attach_guess(Mlp* m);
+    void attach_dataset(Dataset* d, int32_t stride);
     void freeze_limiter(bool frozen) { limiter_frozen_ = frozen; }
 
 private:
@@ -212,6 +222,13 @@ private:
     bool need_grad_ = false;
     bool muscl_ = false;
     bool limiter_frozen_ = false;
+    Mlp* guess_ = nullptr;
+    Dataset* dataset_ = nullptr;
+    int32_t ds_stride_ = 1, ds_phase_ = 0;
+    DevArray<uint16_t> feat_;
+    DevArray<double> du_prev_, gscale_, gpart_;
+    void prepare_guess_inputs();
+    void learn_alloc();
     DevMesh dm_{};
     DevFields df_{};
     SaParams sap_{};

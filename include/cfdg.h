@@ -116,7 +116,8 @@ enum {
 enum {
     CFDG_KCAT_PRIMITIVES = 0, CFDG_KCAT_GRADIENT = 1, CFDG_KCAT_LIMITER = 2, CFDG_KCAT_FACE_FLUX = 3,
     CFDG_KCAT_CELL_GATHER = 4, CFDG_KCAT_JACOBIAN = 5, CFDG_KCAT_LU = 6, CFDG_KCAT_SPMV = 7, CFDG_KCAT_SGS = 8,
-    CFDG_KCAT_KRYLOV = 9, CFDG_KCAT_UPDATE = 10, CFDG_KCAT_TURBULENCE = 11, CFDG_KCAT_COUNT = 12
+    CFDG_KCAT_KRYLOV = 9, CFDG_KCAT_UPDATE = 10, CFDG_KCAT_TURBULENCE = 11,
+    CFDG_KCAT_GUESS = 12, CFDG_KCAT_COUNT = 13
 };
 
 /* ------------------------------------------------------------- structures */
@@ -202,7 +203,8 @@ typedef struct cfdg_step_result {
     double l2[6];              /* L2 residual norms of the evaluated R(U)    */
     double cfl;
     int32_t nvars;
-    int32_t krylov_status, krylov_iterations, guess_used;
+    int32_t krylov_status, krylov_iterations;
+    int32_t guess_used;        /* 0 zero guess, 1 learned guess, 2 learned guess rejected */
     double krylov_initial, krylov_final;
 } cfdg_step_result;
 
@@ -217,6 +219,8 @@ typedef struct cfdg_run_result {
 typedef struct cfdg_solver cfdg_solver;   /* Solver<...> + BackwardEuler     */
 typedef struct cfdg_bsr cfdg_bsr;         /* BsrMatrix + SGS + BiCGSTAB      */
 typedef struct cfdg_host_mesh cfdg_host_mesh;
+typedef struct cfdg_mlp cfdg_mlp;         /* learned initial-guess network    */
+typedef struct cfdg_dataset cfdg_dataset; /* (features, dU) training samples  */
 
 /* ------------------------------------------------------------ library */
 CFDG_API int cfdg_version(void);
@@ -332,6 +336,48 @@ CFDG_API int cfdg_bicgstab(cfdg_bsr* a, int32_t precond, double rel_tol, double 
                   double* x_d, const double* b_d, cfdg_krylov_result* out_h);
 CFDG_API int cfdg_bicgstab_host(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it,
                        double* x_h, const double* b_h, cfdg_krylov_result* out_h);
+
+/* ------------------------------------------------ learned initial guess
+ * Not in the reference (its BiCGSTAB starts from the zero vector,
+ * implicit_euler.hpp:81-92; x0 != 0 is supported by bicgstab.cpp:57-60).
+ * A per-cell MLP (48 features -> 64 -> 64 -> nvars, ReLU, bf16 weights,
+ * fp32 accumulation on the tcgen05 tensor cores) predicts the Newton update
+ * dU0 from the cell's explicit pseudo-time update, state and previous update
+ * and their face-neighbour mean / max; BiCGSTAB then starts from dU0 unless
+ * ||b - A dU0|| >= ||b||, in which case it starts from zero.  Parameters:
+ * fp32, W1[64x48] b1[64] W2[64x64] b2[64] W3[16x64] b3[16] (row-major,
+ * out x in), cfdg_mlp_param_count() values. */
+/* D[128 x n] = A[128 x k] B[n x k]^T on one CTA of tensor cores (bf16 bits,
+ * row-major); n in {16,32,48,64}, k a multiple of 16 <= 128. */
+CFDG_API int cfdg_tc_selftest(int device, int32_t n, int32_t k, const uint16_t* a_h, const uint16_t* b_h,
+                              float* d_h);
+CFDG_API int cfdg_mlp_create(int device, int32_t nvars, uint64_t seed, cfdg_mlp** out);
+CFDG_API int cfdg_mlp_destroy(cfdg_mlp* m);
+CFDG_API int32_t cfdg_mlp_param_count(void);
+CFDG_API int cfdg_mlp_get_params(cfdg_mlp* m, float* out_h, int64_t count);
+CFDG_API int cfdg_mlp_set_params(cfdg_mlp* m, const float* params_h, int64_t count);
+/* out[r*nvars+v] = scale[v] * y_v(row r); features bf16 bits [rows x 48] (device) */
+CFDG_API int cfdg_mlp_forward(cfdg_mlp* m, const uint16_t* feat_d, int64_t rows, const double* scale_d,
+                              double* out_d);
+CFDG_API int cfdg_mlp_forward_host(cfdg_mlp* m, const uint16_t* feat_h, int64_t rows, double* out_h);
+/* mean squared error over rows x nvars of targets t [rows x 16] and its
+ * gradient (cfdg_mlp_param_count() floats); no update */
+CFDG_API int cfdg_mlp_gradient_host(cfdg_mlp* m, const uint16_t* x_h, const float* t_h, int64_t rows,
+                                    float* loss_h, float* grad_h);
+/* Adam over the dataset (shuffled contiguous batches); mean loss of the last epoch */
+CFDG_API int cfdg_mlp_train(cfdg_mlp* m, cfdg_dataset* ds, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                            float* loss_h);
+CFDG_API int cfdg_dataset_create(int device, int32_t nvars, int64_t capacity, cfdg_dataset** out);
+CFDG_API int cfdg_dataset_destroy(cfdg_dataset* d);
+CFDG_API int cfdg_dataset_size(const cfdg_dataset* d, int64_t* size_h);
+CFDG_API int cfdg_dataset_clear(cfdg_dataset* d);
+CFDG_API int cfdg_dataset_append_host(cfdg_dataset* d, const uint16_t* x_h, const float* t_h, int64_t rows);
+CFDG_API int cfdg_dataset_read_host(const cfdg_dataset* d, uint16_t* x_h, float* t_h, int64_t rows);
+/* The solver starts each linear solve from the network's guess (NULL:
+ * zero guess); a dataset receives the features and normalised solved
+ * update of every stride-th cell of every Newton step until it is full. */
+CFDG_API int cfdg_solver_attach_guess(cfdg_solver* s, cfdg_mlp* m);
+CFDG_API int cfdg_solver_attach_dataset(cfdg_solver* s, cfdg_dataset* d, int32_t stride);
 
 #ifdef __cplusplus
 }
