@@ -98,7 +98,7 @@ class KrylovResult(C.Structure):
 class StepResult(C.Structure):
     _fields_ = [("l2", C.c_double * 6), ("cfl", C.c_double), ("nvars", C.c_int32), ("krylov_status", C.c_int32),
                 ("krylov_iterations", C.c_int32), ("guess_used", C.c_int32), ("krylov_initial", C.c_double),
-                ("krylov_final", C.c_double)]
+                ("krylov_final", C.c_double), ("krylov_rhs", C.c_double)]
 
 
 class RunResult(C.Structure):

@@ -143,10 +143,10 @@ def sa_plate(scale: int = 1, seed: int = 2468, iterations: int = 200, mixed: boo
                 {"mach": M, "Re": Re, "T": T, "p": p, "rho": rho, "u": u, "nu_inf": 3.0 * mu / rho})
 
 
-def bump(scale: int = 1, seed: int = 777, iterations: int = 200, mixed: bool = True) -> Case:
+def bump(scale: int = 1, seed: int = 777, iterations: int = 200, mixed: bool = True, mach: float = 0.85) -> Case:
     """Transonic Euler bump, M=0.85, 160x80x80 hex -> 6 tets each (6,144,000 cells)."""
     nx, ny, nz = max(160 // scale, 6), max(80 // scale, 3), max(80 // scale, 3)
-    T, p, M = 288.15, 101325.0, 0.85
+    T, p, M = 288.15, 101325.0, mach
     u = M * sound_speed(T)
     rho = p / (R_GAS * T)
     spec = _spec(2, nx, ny, nz, 3.0, 1.5, 1.5, seed, bump_height=0.1, bump_x0=1.0, bump_x1=2.0, jitter=0.05)

@@ -3,12 +3,17 @@
 // Per cell c and variable v, with e = (dt_c / V_c) * b (the explicit
 // pseudo-time update, b = -R):
 //   g1 = e / s_e, g2 = (U - U_inf) / s_U, g3 = dU_prev / s_d,
-// where s_e, s_d are the RMS over cells of e and of the previous Newton
-// update, and s_U a free-stream scale.  The 48 features are
-//   [g1, g2, g3, mean_nb g1, mean_nb g2, mean_nb g3, max_nb g1, max_nb g2]
-// (8 groups of nvars over the face neighbours, zero padded) in bf16; the
-// network predicts dU / s_e.
+// where s_e and s_d are the RMS over cells of e and of the previous Newton
+// update (one shared value for the momentum vector) and s_U a free-stream
+// scale.  The 48 features are
+//   [g1, g2, g3, mean_nb g1, mean_nb g3, max_nb g1, max_nb g2]
+// (7 groups of nvars over the face neighbours, zero padded) and, last,
+// log10(mean_v s_e / s_d) / 4 and log10(CFL) / 4, in bf16.  The network
+// predicts dU / s_d: the update relative to the previous one, an O(1)
+// quantity in every phase of the convergence.
 #include <cuda_bf16.h>
+
+#include <cmath>
 
 #include "guess.hpp"
 #include "kernels.hpp"
@@ -73,7 +78,8 @@ template <int NV>
 __global__ void __launch_bounds__(128) k_guess_features(DevMesh m, const double* __restrict__ U,
                                                        const double* __restrict__ b, const double* __restrict__ dt,
                                                        const double* __restrict__ du_prev,
-                                                       const double* __restrict__ gscale, uint16_t* __restrict__ feat) {
+                                                       const double* __restrict__ gscale, double lcfl,
+                                                       uint16_t* __restrict__ feat) {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.n) return;
     const int64_t n = m.n;
@@ -94,12 +100,14 @@ __global__ void __launch_bounds__(128) k_guess_features(DevMesh m, const double*
             g3[v] = du_prev[int64_t(k) * NV + v] * isd[v];
         }
     };
-    double f[8 * NV];
-    double s1[NV], s2[NV], s3[NV], mx1[NV], mx2[NV];
+    double f[kMlpIn];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; ++i) f[i] = 0.0;
+    double s1[NV], s3[NV], mx1[NV], mx2[NV];
     groups(c, f, f + NV, f + 2 * NV);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        s1[v] = s2[v] = s3[v] = 0.0;
+        s1[v] = s3[v] = 0.0;
         mx1[v] = mx2[v] = -1.0e300;
     }
     const int32_t j0 = m.c2c_off[c], j1 = m.c2c_off[c + 1];
@@ -109,7 +117,6 @@ __global__ void __launch_bounds__(128) k_guess_features(DevMesh m, const double*
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             s1[v] += g1[v];
-            s2[v] += g2[v];
             s3[v] += g3[v];
             mx1[v] = fmax(mx1[v], g1[v]);
             mx2[v] = fmax(mx2[v], g2[v]);
@@ -119,26 +126,25 @@ __global__ void __launch_bounds__(128) k_guess_features(DevMesh m, const double*
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         f[3 * NV + v] = s1[v] * inv;
-        f[4 * NV + v] = s2[v] * inv;
-        f[5 * NV + v] = s3[v] * inv;
-        f[6 * NV + v] = (j1 > j0) ? mx1[v] : 0.0;
-        f[7 * NV + v] = (j1 > j0) ? mx2[v] : 0.0;
+        f[4 * NV + v] = s3[v] * inv;
+        f[5 * NV + v] = (j1 > j0) ? mx1[v] : 0.0;
+        f[6 * NV + v] = (j1 > j0) ? mx2[v] : 0.0;
     }
+    double ratio = 0.0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) ratio += gscale[v] * isd[v];
+    f[kMlpIn - 2] = 0.25 * log10(fmax(ratio / NV, 1e-30));
+    f[kMlpIn - 1] = lcfl;
     uint32_t packed[kMlpIn / 2];
 #pragma unroll
-    for (int i = 0; i < kMlpIn / 2; ++i) {
-        const int a = 2 * i, bb = 2 * i + 1;
-        const uint16_t lo = (a < 8 * NV) ? bf(f[a]) : uint16_t(0);
-        const uint16_t hi = (bb < 8 * NV) ? bf(f[bb]) : uint16_t(0);
-        packed[i] = uint32_t(lo) | (uint32_t(hi) << 16);
-    }
+    for (int i = 0; i < kMlpIn / 2; ++i) packed[i] = uint32_t(bf(f[2 * i])) | (uint32_t(bf(f[2 * i + 1])) << 16);
     uint4* dst = reinterpret_cast<uint4*>(feat + int64_t(c) * kMlpIn);
 #pragma unroll
     for (int q = 0; q < kMlpIn / 8; ++q)
         dst[q] = make_uint4(packed[4 * q], packed[4 * q + 1], packed[4 * q + 2], packed[4 * q + 3]);
 }
 
-// Samples c = phase + k * stride: features row and target dU / s_e.
+// Samples c = phase + k * stride: features row and target dU / s_d.
 __global__ void k_guess_append(int32_t n, int nv, int32_t stride, int32_t phase, int64_t count,
                                const uint16_t* __restrict__ feat, const double* __restrict__ du,
                                const double* __restrict__ gscale, uint16_t* __restrict__ X, float* __restrict__ T) {
@@ -150,7 +156,7 @@ __global__ void k_guess_append(int32_t n, int nv, int32_t stride, int32_t phase,
 #pragma unroll
     for (int q = 0; q < kMlpIn / 8; ++q) dst[q] = src[q];
     for (int v = 0; v < kMlpOut; ++v)
-        T[k * kMlpOut + v] = (v < nv) ? static_cast<float>(du[c * nv + v] / gscale[v]) : 0.0f;
+        T[k * kMlpOut + v] = (v < nv) ? static_cast<float>(du[c * nv + v] / gscale[8 + v]) : 0.0f;
 }
 
 }  // namespace
@@ -170,10 +176,11 @@ void launch_guess_scales(int32_t n, int nv, const double* b, const double* dt, c
 }
 
 void launch_guess_features(const DevMesh& m, int nv, const double* U, const double* b, const double* dt,
-                           const double* du_prev, const double* gscale, uint16_t* feat, cudaStream_t s) {
+                           const double* du_prev, const double* gscale, double cfl, uint16_t* feat, cudaStream_t s) {
     const unsigned gr = grid_for(m.n, 128);
-    if (nv == 6) k_guess_features<6><<<gr, 128, 0, s>>>(m, U, b, dt, du_prev, gscale, feat);
-    else k_guess_features<5><<<gr, 128, 0, s>>>(m, U, b, dt, du_prev, gscale, feat);
+    const double lcfl = 0.25 * std::log10(cfl > 0.0 ? cfl : 1.0);
+    if (nv == 6) k_guess_features<6><<<gr, 128, 0, s>>>(m, U, b, dt, du_prev, gscale, lcfl, feat);
+    else k_guess_features<5><<<gr, 128, 0, s>>>(m, U, b, dt, du_prev, gscale, lcfl, feat);
 }
 
 void launch_guess_append(int32_t n, int nv, int32_t stride, int32_t phase, int64_t count, const uint16_t* feat,

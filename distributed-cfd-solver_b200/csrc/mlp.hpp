@@ -11,7 +11,7 @@
 
 namespace cfdg {
 
-constexpr int kMlpIn = 48;    // features per cell (8 groups of nvars, zero padded)
+constexpr int kMlpIn = 48;    // features per cell (7 groups of nvars + log CFL, zero padded)
 constexpr int kMlpHid = 64;   // hidden width
 constexpr int kMlpOut = 16;   // outputs (nvars used, zero padded)
 constexpr int kMlpTile = 128; // cells per tensor-core tile (MMA M)

@@ -522,6 +522,7 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
     cuda_check(cudaMemcpyAsync(ks_host_, ks_.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, stream_), "D2H");
     cuda_check(cudaStreamSynchronize(stream_), "krylov sync");
     last_guess_ = guess ? ks_host_->guess : 0;
+    last_bnorm_ = ks_host_->bnorm;
     cfdg_krylov_result res{};
     switch (ks_host_->state) {
         case KS_CONVERGED: res.status = CFDG_KRYLOV_CONVERGED; break;
@@ -948,6 +949,7 @@ void Solver::sizes(int64_t* out) const {
 // Solver::init_fields (solver.hpp:507-544): primitives_rhop_to_conserved of
 // the [initial] state on every cell.
 void Solver::init_fields() {
+    have_prev_ = false;
     const double rho = cfg_.init_rho, p = cfg_.init_p;
     const double u = cfg_.init_velocity[0], v = cfg_.init_velocity[1], w = cfg_.init_velocity[2];
     const double T = p / (rho * gas_.R);
@@ -968,6 +970,7 @@ void Solver::init_fields() {
 
 void Solver::set_state_host(const double* u, int64_t ld) {
     if (ld < dm_.n) throw Failure{CFDG_ERR_INVALID, "leading dimension smaller than n_cells"};
+    have_prev_ = false;
     for (int v = 0; v < nv_; ++v)
         cuda_check(cudaMemcpyAsync(U_.p + static_cast<std::size_t>(v) * dm_.n, u + v * ld, sizeof(double) * dm_.n,
                                    cudaMemcpyHostToDevice, stream_),
@@ -1067,6 +1070,7 @@ void Solver::evaluate_residual() {
 
 void Solver::compute_dt(double cfl) {
     if (!(cfl > 0.0)) throw Failure{CFDG_ERR_INVALID, "CFL must be positive"};
+    cfl_now_ = cfl;
     ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, ab_.dt_rhs);
     launch_dt_rhs(dm_, df_, nv_, cfl, b_.p, du_.p, stream_);
     cuda_check(cudaGetLastError(), "dt launch");
@@ -1101,14 +1105,18 @@ void Solver::assemble_jacobian() {
 cfdg_krylov_result Solver::linear_solve() {
     if (cfg_.precond == CFDG_PC_SGS) sys_->sgs_setup(cfg_.sgs_ordering, std::max(cfg_.sgs_sweeps, 1));
     if (guess_ || dataset_) prepare_guess_inputs();
-    if (guess_) {
+    // the network predicts the update relative to the previous one: no
+    // guess before a previous update exists
+    const bool use_guess = guess_ && have_prev_;
+    if (use_guess) {
         ProfScope ps(&prof_, CFDG_KCAT_GUESS, stream_, 1, double(dm_.n) * (kMlpIn * 2.0 + nv_ * 8.0));
-        guess_->forward(feat_.p, dm_.n, gscale_.p, du_.p, stream_);
+        guess_->forward(feat_.p, dm_.n, gscale_.p + 8, du_.p, stream_);
     } else {
         cuda_check(cudaMemsetAsync(du_.p, 0, du_.count * sizeof(double), stream_), "memset");
     }
     last_krylov_ = sys_->bicgstab(cfg_.precond, cfg_.lin_rel_tol, cfg_.lin_abs_tol, cfg_.lin_max_iterations, du_.p,
-                                  b_.p, guess_ != nullptr);
+                                  b_.p, use_guess);
+    last_used_guess_ = use_guess;
     return last_krylov_;
 }
 
@@ -1144,7 +1152,7 @@ void Solver::prepare_guess_inputs() {
                  double(dm_.n) * (nv_ * 8.0 * 4 + 16.0) +
                      double(dm_.n) * (kMlpIn * 2.0 + 8.0 * (nv_ * 3 + 2)) + double(c2c_.count) * 4.0);
     launch_guess_scales(dm_.n, nv_, b_.p, dt_.p, vol_.p, du_prev_.p, gpart_.p, gscale_.p, stream_);
-    launch_guess_features(dm_, nv_, U_.p, b_.p, dt_.p, du_prev_.p, gscale_.p, feat_.p, stream_);
+    launch_guess_features(dm_, nv_, U_.p, b_.p, dt_.p, du_prev_.p, gscale_.p, cfl_now_, feat_.p, stream_);
     cuda_check(cudaGetLastError(), "guess launch");
 }
 
@@ -1182,7 +1190,7 @@ cfdg_step_result Solver::newton_step(double cfl) {
     compute_dt(cfl);
     assemble_jacobian();
     const cfdg_krylov_result kr = linear_solve();
-    if (dataset_) {
+    if (dataset_ && have_prev_) {
         const int64_t want = (int64_t(dm_.n) - ds_phase_ + ds_stride_ - 1) / ds_stride_;
         const int64_t at = dataset_->size();
         const int64_t got = dataset_->reserve(want);
@@ -1197,9 +1205,11 @@ cfdg_step_result Solver::newton_step(double cfl) {
         ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, ab_.state_update);
         launch_state_update(dm_, U_.p, du_.p, nv_, stream_);
     }
-    if (guess_ || dataset_)
+    if (guess_ || dataset_) {
         cuda_check(cudaMemcpyAsync(du_prev_.p, du_.p, du_.count * sizeof(double), cudaMemcpyDeviceToDevice, stream_),
                    "D2D");
+        have_prev_ = true;
+    }
     residual_norms(r.l2);
     r.cfl = cfl;
     r.nvars = nv_;
@@ -1207,7 +1217,8 @@ cfdg_step_result Solver::newton_step(double cfl) {
     r.krylov_iterations = kr.iterations;
     r.krylov_initial = kr.initial_residual;
     r.krylov_final = kr.final_residual;
-    r.guess_used = guess_ ? sys_->last_guess() : 0;
+    r.guess_used = last_used_guess_ ? sys_->last_guess() : 0;
+    r.krylov_rhs = sys_->last_bnorm();
     return r;
 }
 

@@ -139,6 +139,7 @@ public:
     cfdg_krylov_result bicgstab(int precond, double rel_tol, double abs_tol, int max_it, double* x, const double* b,
                                 bool guess = false);
     int last_guess() const { return last_guess_; }
+    double last_bnorm() const { return last_bnorm_; }
     int groups_fwd() const { return static_cast<int>(fwd_off_.size()) - 1; }
     int groups_bwd() const { return static_cast<int>(bwd_off_.size()) - 1; }
     int64_t launches() const { return prof_->launches; }
@@ -164,6 +165,7 @@ private:
     DevArray<int> err_;
     int ordering_ = -1, sweeps_ = 1;
     int last_guess_ = 0;
+    double last_bnorm_ = 0.0;
     bool lu_ready_ = false;
     std::vector<int32_t> fwd_off_, bwd_off_;
     std::vector<double> fwd_bytes_[2], bwd_bytes_[2];  // algorithmic bytes of one pass, mode 0 / mode 1
@@ -227,6 +229,8 @@ private:
     int32_t ds_stride_ = 1, ds_phase_ = 0;
     DevArray<uint16_t> feat_;
     DevArray<double> du_prev_, gscale_, gpart_;
+    double cfl_now_ = 1.0;
+    bool have_prev_ = false, last_used_guess_ = false;
     void prepare_guess_inputs();
     void learn_alloc();
     DevMesh dm_{};

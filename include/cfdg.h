@@ -206,6 +206,7 @@ typedef struct cfdg_step_result {
     int32_t krylov_status, krylov_iterations;
     int32_t guess_used;        /* 0 zero guess, 1 learned guess, 2 learned guess rejected */
     double krylov_initial, krylov_final;
+    double krylov_rhs;         /* ||b||: krylov_initial / krylov_rhs < 1 when the guess helped */
 } cfdg_step_result;
 
 typedef struct cfdg_run_result {
