@@ -13,6 +13,16 @@ pinned host memory and copied back every step.  Under torchrun each rank
 runs an independent replica on its own GPU (no data-path collective): value
 is the sum over ranks of cells x steps divided by the maximum rank time.
 
+The second half of the metric, time to a 1e-8 residual drop, is the
+`time_to_1e8` object (single GPU): the transonic Euler bump (M = 0.85; the
+160x80x80x6-tet mesh divided by --converge-scale per direction, 2 by
+default: 768,000 cells) run to a 1e-8 residual drop three ways: plain FP64,
+mixed precision (FP32 Jacobian / SGS / SpMV), and mixed precision with the
+learned initial guess.  The network is trained on the GPU first, by the
+library's own tcgen05 kernels, on samples the solver writes out while it
+converges the bump at M = 0.8 and 0.9 on a mesh twice as coarse; that
+training is timed separately and is not part of the time to solution.
+
 `--impl reference` times the reference solver's own CPU implementation
 (built from its sources, oracle/_ref) on the same workload and metric.
 """
@@ -311,10 +321,60 @@ def run_ours(args):
                 "roofline": roof}
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = _cpu_baseline(cb, case, mesh, args.cpu_steps)
+        if not args.no_converge and world == 1:
+            line["time_to_1e8"] = _time_to_converge(cb, args.converge_scale)
         print(json.dumps(line))
     s.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def _time_to_converge(cb, scale: int):
+    """Wall time of run_steady to a 1e-8 residual drop on the bump: FP64,
+    mixed, mixed + learned guess (network trained first on other flows)."""
+    t0 = time.perf_counter()
+    ds = cb.Dataset(5, 6_000_000)
+    collect = []
+    for mach in (0.8, 0.9):
+        case = cb.cases.bump(scale=2 * scale, mixed=True, mach=mach, iterations=2000)
+        mesh = cb.HostMesh(case.spec)
+        stride = max(1, (mesh.n_cells * 1000) // 3_000_000)
+        with cb.Solver(mesh, case.cfg, case.bcs) as s:
+            s.init_fields()
+            s.attach_dataset(ds, stride)
+            r = s.run_steady()
+            collect.append({"mach": mach, "cells": mesh.n_cells, "iterations": int(r.iterations),
+                            "converged": bool(r.converged)})
+    t_collect = time.perf_counter() - t0
+    net = cb.Mlp(5, seed=5)
+    t1 = time.perf_counter()
+    loss = net.train(ds, epochs=20, batch=8192, lr=1e-3)
+    t_train = time.perf_counter() - t1
+    case = cb.cases.bump(scale=scale, iterations=4000)
+    mesh = cb.HostMesh(case.spec)
+    out = {"workload": f"transonic Euler bump M=0.85, {mesh.n_cells} tets (160x80x80x6 / {scale}^3), "
+                       f"run_steady to a 1e-8 drop of max(mass, |momentum|, energy) L2 vs its running maximum",
+           "training": {"samples": len(ds), "epochs": 20, "final_loss": round(loss, 6),
+                        "collect_s": round(t_collect, 2), "train_s": round(t_train, 3), "runs": collect}}
+    fields = {}
+    for name, prec, learned in (("fp64", 0, False), ("mixed", 1, False), ("mixed_learned", 1, True)):
+        c = cb.cases.bump(scale=scale, iterations=4000)
+        c.cfg.precision = prec
+        with cb.Solver(mesh, c.cfg, c.bcs) as s:
+            s.init_fields()
+            if learned:
+                s.attach_guess(net)
+            r = s.run_steady()
+            fields[name] = s.get(cb.FIELD_U).reshape(5, -1)
+        out[name] = {"seconds": round(r.seconds, 3), "iterations": int(r.iterations), "converged": bool(r.converged),
+                     "rel": float(r.rel), "krylov_iterations": int(r.krylov_iterations_total)}
+    ref = fields["fp64"]
+    for name in ("mixed", "mixed_learned"):
+        out[name]["field_rel_l2_vs_fp64"] = [
+            float("%.3g" % (np.linalg.norm(fields[name][v] - ref[v]) / max(np.linalg.norm(ref[v]), 1e-300)))
+            for v in (0, 1, 2, 4)]
+    out["speedup_mixed_learned_vs_fp64"] = round(out["fp64"]["seconds"] / out["mixed_learned"]["seconds"], 3)
+    return out
 
 
 def _cfl(case, it):
@@ -333,6 +393,8 @@ def main():
     ap.add_argument("--scale", type=int, default=1, help="divide each mesh dimension (profiling runs)")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8 runs")
+    ap.add_argument("--converge-scale", type=int, default=2, help="bump mesh divisor of the time-to-1e-8 runs")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
