@@ -36,7 +36,12 @@ struct DevMesh {
     const BcPatch* patches;
     int32_t n_patches;
     const double* wall_dist;             // n (SA)
+    // linear-system row of each cell (n) when the BSR matrix and its vectors
+    // are stored in colour order; null: row = cell
+    const int32_t* row_of;
 };
+
+__host__ __device__ inline int32_t row_index(const DevMesh& m, int32_t c) { return m.row_of ? m.row_of[c] : c; }
 
 struct GasParams {
     double gamma, R, cv, cp, prandtl, prandtl_turb;

@@ -14,12 +14,13 @@
 namespace cfdg {
 
 int guess_sum_blocks(int32_t n);
-void launch_guess_scales(int32_t n, int nv, const double* b, const double* dt, const double* vol,
-                         const double* du_prev, double* partials, double* gscale, cudaStream_t s);
+void launch_guess_scales(int32_t n, const int32_t* row_of, int nv, const double* b, const double* dt,
+                         const double* vol, const double* du_prev, double* partials, double* gscale, cudaStream_t s);
 void launch_guess_features(const DevMesh& m, int nv, const double* U, const double* b, const double* dt,
                            const double* du_prev, const double* gscale, double cfl, uint16_t* feat, cudaStream_t s);
-void launch_guess_append(int32_t n, int nv, int32_t stride, int32_t phase, int64_t count, const uint16_t* feat,
-                         const double* du, const double* gscale, uint16_t* X, float* T, cudaStream_t s);
+void launch_guess_append(int32_t n, const int32_t* row_of, int nv, int32_t stride, int32_t phase, int64_t count,
+                         const uint16_t* feat, const double* du, const double* gscale, uint16_t* X, float* T,
+                         cudaStream_t s);
 
 class Dataset;
 

@@ -26,7 +26,8 @@ namespace {
 constexpr int kSumThreads = 256;
 
 template <int NV>
-__global__ void __launch_bounds__(kSumThreads) k_guess_sums(int32_t n, const double* __restrict__ b,
+__global__ void __launch_bounds__(kSumThreads) k_guess_sums(int32_t n, const int32_t* __restrict__ row_of,
+                                                           const double* __restrict__ b,
                                                            const double* __restrict__ dt,
                                                            const double* __restrict__ vol,
                                                            const double* __restrict__ du_prev,
@@ -37,10 +38,11 @@ __global__ void __launch_bounds__(kSumThreads) k_guess_sums(int32_t n, const dou
     for (int k = 0; k < 2 * NV; ++k) acc[k] = 0.0;
     if (c < n) {
         const double w = dt[c] / vol[c];
+        const int64_t r = row_of ? row_of[c] : c;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const double e = w * b[int64_t(c) * NV + v];
-            const double d = du_prev[int64_t(c) * NV + v];
+            const double e = w * b[r * NV + v];
+            const double d = du_prev[r * NV + v];
             acc[v] = e * e;
             acc[NV + v] = d * d;
         }
@@ -93,11 +95,12 @@ __global__ void __launch_bounds__(128) k_guess_features(DevMesh m, const double*
     }
     auto groups = [&](int32_t k, double* g1, double* g2, double* g3) {
         const double w = dt[k] / m.vol[k];
+        const int64_t r = row_index(m, k);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            g1[v] = w * b[int64_t(k) * NV + v] * ise[v];
+            g1[v] = w * b[r * NV + v] * ise[v];
             g2[v] = (U[v * n + k] - uinf[v]) * isu[v];
-            g3[v] = du_prev[int64_t(k) * NV + v] * isd[v];
+            g3[v] = du_prev[r * NV + v] * isd[v];
         }
     };
     double f[kMlpIn];
@@ -138,19 +141,22 @@ __global__ void __launch_bounds__(128) k_guess_features(DevMesh m, const double*
     uint32_t packed[kMlpIn / 2];
 #pragma unroll
     for (int i = 0; i < kMlpIn / 2; ++i) packed[i] = uint32_t(bf(f[2 * i])) | (uint32_t(bf(f[2 * i + 1])) << 16);
-    uint4* dst = reinterpret_cast<uint4*>(feat + int64_t(c) * kMlpIn);
+    // the feature row of a cell is its linear-system row, so that the
+    // network's outputs land in the layout of the Krylov vectors
+    uint4* dst = reinterpret_cast<uint4*>(feat + int64_t(row_index(m, c)) * kMlpIn);
 #pragma unroll
     for (int q = 0; q < kMlpIn / 8; ++q)
         dst[q] = make_uint4(packed[4 * q], packed[4 * q + 1], packed[4 * q + 2], packed[4 * q + 3]);
 }
 
 // Samples c = phase + k * stride: features row and target dU / s_d.
-__global__ void k_guess_append(int32_t n, int nv, int32_t stride, int32_t phase, int64_t count,
-                               const uint16_t* __restrict__ feat, const double* __restrict__ du,
+__global__ void k_guess_append(int32_t n, const int32_t* __restrict__ row_of, int nv, int32_t stride, int32_t phase,
+                               int64_t count, const uint16_t* __restrict__ feat, const double* __restrict__ du,
                                const double* __restrict__ gscale, uint16_t* __restrict__ X, float* __restrict__ T) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= count) return;
-    const int64_t c = phase + k * stride;
+    const int64_t c0 = phase + k * stride;
+    const int64_t c = row_of ? row_of[c0] : c0;
     const uint4* src = reinterpret_cast<const uint4*>(feat + c * kMlpIn);
     uint4* dst = reinterpret_cast<uint4*>(X + k * kMlpIn);
 #pragma unroll
@@ -163,14 +169,14 @@ __global__ void k_guess_append(int32_t n, int nv, int32_t stride, int32_t phase,
 
 int guess_sum_blocks(int32_t n) { return static_cast<int>((int64_t(n) + kSumThreads - 1) / kSumThreads); }
 
-void launch_guess_scales(int32_t n, int nv, const double* b, const double* dt, const double* vol,
-                         const double* du_prev, double* partials, double* gscale, cudaStream_t s) {
+void launch_guess_scales(int32_t n, const int32_t* row_of, int nv, const double* b, const double* dt,
+                         const double* vol, const double* du_prev, double* partials, double* gscale, cudaStream_t s) {
     const int nb = guess_sum_blocks(n);
     if (nv == 6) {
-        k_guess_sums<6><<<nb, kSumThreads, 0, s>>>(n, b, dt, vol, du_prev, partials);
+        k_guess_sums<6><<<nb, kSumThreads, 0, s>>>(n, row_of, b, dt, vol, du_prev, partials);
         k_guess_scales<6><<<1, 32, 0, s>>>(n, partials, nb, gscale);
     } else {
-        k_guess_sums<5><<<nb, kSumThreads, 0, s>>>(n, b, dt, vol, du_prev, partials);
+        k_guess_sums<5><<<nb, kSumThreads, 0, s>>>(n, row_of, b, dt, vol, du_prev, partials);
         k_guess_scales<5><<<1, 32, 0, s>>>(n, partials, nb, gscale);
     }
 }
@@ -183,10 +189,11 @@ void launch_guess_features(const DevMesh& m, int nv, const double* U, const doub
     else k_guess_features<5><<<gr, 128, 0, s>>>(m, U, b, dt, du_prev, gscale, lcfl, feat);
 }
 
-void launch_guess_append(int32_t n, int nv, int32_t stride, int32_t phase, int64_t count, const uint16_t* feat,
-                         const double* du, const double* gscale, uint16_t* X, float* T, cudaStream_t s) {
+void launch_guess_append(int32_t n, const int32_t* row_of, int nv, int32_t stride, int32_t phase, int64_t count,
+                         const uint16_t* feat, const double* du, const double* gscale, uint16_t* X, float* T,
+                         cudaStream_t s) {
     if (count <= 0) return;
-    k_guess_append<<<grid_for(count, 128), 128, 0, s>>>(n, nv, stride, phase, count, feat, du, gscale, X, T);
+    k_guess_append<<<grid_for(count, 128), 128, 0, s>>>(n, row_of, nv, stride, phase, count, feat, du, gscale, X, T);
 }
 
 }  // namespace cfdg

@@ -137,12 +137,13 @@ __global__ void __launch_bounds__(256) k_jac_diag(DevMesh m, const double* __res
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= int64_t(m.n) * 25) return;
     const int32_t c = static_cast<int32_t>(t / 25);
+    const int32_t row = row_index(m, c);
     const int e = static_cast<int>(t % 25);
     const int er = e / 5, ec = e % 5;
     const int eb = er * BS + ec;
-    const int32_t d = js.diag[c];
+    const int32_t d = js.diag[row];
     double v = 0.0;
-    for (int32_t k = js.row_ptr[c]; k < js.row_ptr[c + 1]; ++k) {
+    for (int32_t k = js.row_ptr[row]; k < js.row_ptr[row + 1]; ++k) {
         if (k == d) continue;
         v -= static_cast<double>(vals[int64_t(js.trans[k]) * (BS * BS) + eb]);
     }

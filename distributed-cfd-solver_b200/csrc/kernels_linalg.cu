@@ -8,6 +8,8 @@
 //   lu_solve_block<BS>    include/cfd/linalg/bsr_helpers.hpp:324-353
 //   bsr_sgs_sweep<BS>     include/cfd/linalg/bsr_helpers.hpp:389-435
 //   BiCGSTAB::solve       src/linalg/bicgstab.cpp:42-201
+#include <algorithm>
+
 #include "kernels.hpp"
 #include "krylov.hpp"
 
@@ -130,8 +132,9 @@ __global__ void k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu
 
 // Pivoted forward/backward substitution of one block (lu_solve_block) in
 // registers; b holds the right-hand side on entry and the solution on exit.
-template <typename MT, int BS>
+template <typename MT, int BS, bool SMEM = false>
 __device__ __forceinline__ void lu_solve(const MT* __restrict__ lu, const int8_t* __restrict__ piv, double (&b)[BS]) {
+    auto L = [&](int idx) -> double { return SMEM ? static_cast<double>(lu[idx]) : ld(lu + idx); };
 #pragma unroll
     for (int k = 0; k < BS; ++k) {
         const int p = piv[k];
@@ -149,15 +152,15 @@ __device__ __forceinline__ void lu_solve(const MT* __restrict__ lu, const int8_t
     for (int i = 1; i < BS; ++i) {
         double s = b[i];
 #pragma unroll
-        for (int j = 0; j < i; ++j) s -= ld(lu + i * BS + j) * b[j];
+        for (int j = 0; j < i; ++j) s -= L(i * BS + j) * b[j];
         b[i] = s;
     }
 #pragma unroll
     for (int i = BS - 1; i >= 0; --i) {
         double s = b[i];
 #pragma unroll
-        for (int j = i + 1; j < BS; ++j) s -= ld(lu + i * BS + j) * b[j];
-        b[i] = s / ld(lu + i * BS + i);
+        for (int j = i + 1; j < BS; ++j) s -= L(i * BS + j) * b[j];
+        b[i] = s / L(i * BS + i);
     }
 }
 
@@ -169,8 +172,8 @@ __device__ __forceinline__ void lu_solve(const MT* __restrict__ lu, const int8_t
 template <typename MT, int BS, int MODE>
 __global__ void __launch_bounds__(256) k_sgs_rows(BsrView A, const MT* __restrict__ vals, const MT* __restrict__ lu,
                                                   const int8_t* __restrict__ piv, const int32_t* __restrict__ rows,
-                                                  int32_t n_rows, const double* __restrict__ r, double* __restrict__ z,
-                                                  const int* __restrict__ active) {
+                                                  int32_t row0, int32_t n_rows, const double* __restrict__ r,
+                                                  double* __restrict__ z, const int* __restrict__ active) {
     if (active && *active != 0) return;
     constexpr int GPW = 32 / BS;
     const int lane = threadIdx.x & 31;
@@ -181,7 +184,7 @@ __global__ void __launch_bounds__(256) k_sgs_rows(BsrView A, const MT* __restric
     int32_t i = 0;
     double s = 0.0;
     if (act) {
-        i = rows[slot];
+        i = rows ? rows[slot] : row0 + static_cast<int32_t>(slot);  // null: a contiguous group
         s = r[int64_t(i) * BS + ii];
         if (MODE == 0) {
             const int32_t d = A.diag[i];
@@ -468,14 +471,15 @@ void launch_lu_setup(const BsrView& A, const MT* vals, MT* lu, int8_t* piv, int*
 
 template <typename MT>
 void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* rows,
-                        int32_t n_rows, const double* r, double* z, int mode, const int* active, cudaStream_t s) {
+                        int32_t row0, int32_t n_rows, const double* r, double* z, int mode, const int* active,
+                        cudaStream_t s) {
     if (n_rows <= 0) return;
     const int gpw = 32 / A.bs;
     const int64_t warps = (int64_t(n_rows) + gpw - 1) / gpw;
     const unsigned gr = grid_for(warps * 32, 256);
 #define CFDG_SGS(BS)                                                                                          \
-    if (mode == 0) k_sgs_rows<MT, BS, 0><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, n_rows, r, z, active); \
-    else k_sgs_rows<MT, BS, 1><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, n_rows, r, z, active)
+    if (mode == 0) k_sgs_rows<MT, BS, 0><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active); \
+    else k_sgs_rows<MT, BS, 1><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active)
     switch (A.bs) {
         case 1: CFDG_SGS(1); break;
         case 3: CFDG_SGS(3); break;
@@ -549,8 +553,8 @@ template void launch_spmv_ex<float>(const BsrView&, const float*, const double*,
 template void launch_lu_setup<double>(const BsrView&, const double*, double*, int8_t*, int*, cudaStream_t);
 template void launch_lu_setup<float>(const BsrView&, const float*, float*, int8_t*, int*, cudaStream_t);
 template void launch_sgs_rows_ex<double>(const BsrView&, const double*, const double*, const int8_t*, const int32_t*,
-                                         int32_t, const double*, double*, int, const int*, cudaStream_t);
+                                         int32_t, int32_t, const double*, double*, int, const int*, cudaStream_t);
 template void launch_sgs_rows_ex<float>(const BsrView&, const float*, const float*, const int8_t*, const int32_t*,
-                                        int32_t, const double*, double*, int, const int*, cudaStream_t);
+                                        int32_t, int32_t, const double*, double*, int, const int*, cudaStream_t);
 
 }  // namespace cfdg

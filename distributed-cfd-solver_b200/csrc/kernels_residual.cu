@@ -275,10 +275,11 @@ __global__ void k_dt_rhs(DevMesh m, DevFields f, double cfl, double* __restrict_
     f.dt[c] = cfl * m.vol[c] / l;
     f.alpha[c] = (l * inv_cfl) + (m.vol[c] * 0.0);
     if (b) {
+        const int64_t r = row_index(m, c);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            b[int64_t(c) * NV + v] = -f.res[v * n + c];
-            du[int64_t(c) * NV + v] = 0.0;
+            b[r * NV + v] = -f.res[v * n + c];
+            du[r * NV + v] = 0.0;
         }
     }
 }
@@ -290,9 +291,10 @@ __global__ void k_state_update(DevMesh m, double* __restrict__ U, const double* 
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.n) return;
     const int64_t n = m.n;
+    const int64_t r = row_index(m, c);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        double x = U[v * n + c] + du[int64_t(c) * NV + v];
+        double x = U[v * n + c] + du[r * NV + v];
         if (v == 5 && x < 0.0) x = 0.0;
         U[v * n + c] = x;
     }

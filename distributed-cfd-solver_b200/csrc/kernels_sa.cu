@@ -193,16 +193,17 @@ __global__ void k_sa_jac_diag(DevMesh m, const double* __restrict__ alpha, JacSt
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= int64_t(m.n) * 11) return;
     const int32_t c = static_cast<int32_t>(t / 11);
+    const int32_t row = row_index(m, c);
     const int e = static_cast<int>(t % 11);  // 0..4: [5][e], 5..9: [e-5][5], 10: [5][5]
-    MT* d = vals + int64_t(js.diag[c]) * 36;
+    MT* d = vals + int64_t(js.diag[row]) * 36;
     if (e < 5) {
         d[30 + e] = MT(0);
     } else if (e < 10) {
         d[(e - 5) * 6 + 5] = MT(0);
     } else {
-        const int32_t dk = js.diag[c];
+        const int32_t dk = js.diag[row];
         double v = 0.0;
-        for (int32_t k = js.row_ptr[c]; k < js.row_ptr[c + 1]; ++k) {
+        for (int32_t k = js.row_ptr[row]; k < js.row_ptr[row + 1]; ++k) {
             if (k == dk) continue;
             v -= static_cast<double>(vals[int64_t(js.trans[k]) * 36 + 35]);
         }

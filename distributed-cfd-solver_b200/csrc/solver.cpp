@@ -325,6 +325,20 @@ void BsrSystem::build_ordering(int ordering) {
     std::vector<int32_t> fr, br;
     group(fwd_key, fwd_off_, fr);
     group(bwd_key, bwd_off_, br);
+    // groups whose rows are consecutive (a colour-ordered matrix) run
+    // without the row list
+    auto contiguous = [&](const std::vector<int32_t>& off, const std::vector<int32_t>& rows,
+                          std::vector<int32_t>& first) {
+        const int ng = static_cast<int>(off.size()) - 1;
+        first.assign(ng, -1);
+        for (int g = 0; g < ng; ++g) {
+            bool ok = off[g + 1] > off[g];
+            for (int32_t q = off[g] + 1; ok && q < off[g + 1]; ++q) ok = rows[q] == rows[q - 1] + 1;
+            if (ok) first[g] = rows[off[g]];
+        }
+    };
+    contiguous(fwd_off_, fr, fwd_first_);
+    contiguous(bwd_off_, br, bwd_first_);
     // Unique-touch bytes of one pass over a group: row list, row pointers,
     // diagonal index, off-diagonal blocks + columns, LU + pivots, r, z write,
     // and each distinct neighbour z block once.
@@ -411,14 +425,16 @@ void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, doubl
                 if (sw == 0 && g == 0) mode = 1; // all neighbours still zero
             }
             ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, fwd_bytes_[mode][g]);
-            launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, fwd_rows_.p + fwd_off_[g], fwd_off_[g + 1] - fwd_off_[g], r,
-                                   z, mode, active, stream_);
+            const bool cg = fwd_first_[g] >= 0;
+            launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, cg ? nullptr : fwd_rows_.p + fwd_off_[g], cg ? fwd_first_[g] : 0,
+                                   fwd_off_[g + 1] - fwd_off_[g], r, z, mode, active, stream_);
         }
         for (int g = 0; g < nbk; ++g) {
             if (color && g == 0) continue;  // first backward colour == last forward colour
             ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, bwd_bytes_[0][g]);
-            launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, bwd_rows_.p + bwd_off_[g], bwd_off_[g + 1] - bwd_off_[g], r,
-                                   z, 0, active, stream_);
+            const bool cg = bwd_first_[g] >= 0;
+            launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, cg ? nullptr : bwd_rows_.p + bwd_off_[g], cg ? bwd_first_[g] : 0,
+                                   bwd_off_[g + 1] - bwd_off_[g], r, z, 0, active, stream_);
         }
     }
 }
@@ -818,15 +834,50 @@ void Solver::setup_bcs(const cfdg_bc_desc* bcs, int n_bcs, const HostMesh& hm) {
 
 void Solver::setup_matrix(const HostMesh& hm, const Csr& c2c) {
     const int32_t n = hm.n_cells;
+    // Multicolour SGS: store the system in colour order (greedy colouring in
+    // cell order, as the preconditioner's own), so that every colour pass
+    // streams one contiguous range of block rows.  The level-scheduled
+    // (parity) ordering keeps the reference's cell order.
+    row_of_h_.clear();
+    cell_of_h_.clear();
+    if (cfg_.precond == CFDG_PC_SGS && cfg_.sgs_ordering == CFDG_SGS_COLOR) {
+        std::vector<int32_t> color(static_cast<std::size_t>(n), -1);
+        std::vector<char> used;
+        int32_t ncol = 0;
+        for (int32_t c = 0; c < n; ++c) {
+            used.assign(static_cast<std::size_t>(ncol) + 1, 0);
+            for (int32_t k = c2c.off[c]; k < c2c.off[c + 1]; ++k) {
+                const int32_t j = c2c.val[k];
+                if (color[j] >= 0) used[color[j]] = 1;
+            }
+            int32_t col = 0;
+            while (used[col]) ++col;
+            color[c] = col;
+            ncol = std::max(ncol, col + 1);
+        }
+        std::vector<int32_t> start(static_cast<std::size_t>(ncol) + 1, 0);
+        for (int32_t c = 0; c < n; ++c) ++start[color[c] + 1];
+        for (int32_t g = 0; g < ncol; ++g) start[g + 1] += start[g];
+        row_of_h_.resize(n);
+        cell_of_h_.resize(n);
+        for (int32_t c = 0; c < n; ++c) {
+            const int32_t r = start[color[c]]++;
+            row_of_h_[c] = r;
+            cell_of_h_[r] = c;
+        }
+    }
+    const bool perm = !row_of_h_.empty();
+    auto R = [&](int32_t c) { return perm ? row_of_h_[c] : c; };
     // bsr_assemble (linalg/bsr_helpers.hpp:16-59): self + face neighbours, sorted.
     std::vector<int32_t> row_ptr(static_cast<std::size_t>(n) + 1, 0), cols;
     cols.reserve(c2c.val.size() + n);
-    for (int32_t c = 0; c < n; ++c) {
-        const std::size_t start = cols.size();
-        cols.push_back(c);
-        for (int32_t k = c2c.off[c]; k < c2c.off[c + 1]; ++k) cols.push_back(c2c.val[k]);
-        std::sort(cols.begin() + start, cols.end());
-        row_ptr[c + 1] = static_cast<int32_t>(cols.size());
+    for (int32_t r = 0; r < n; ++r) {
+        const int32_t c = perm ? cell_of_h_[r] : r;
+        const std::size_t s0 = cols.size();
+        cols.push_back(r);
+        for (int32_t k = c2c.off[c]; k < c2c.off[c + 1]; ++k) cols.push_back(R(c2c.val[k]));
+        std::sort(cols.begin() + s0, cols.end());
+        row_ptr[r + 1] = static_cast<int32_t>(cols.size());
     }
     sys_ = std::make_unique<BsrSystem>(device_, n, nv_, row_ptr.data(), cols.data(), cfg_.precision, stream_);
     auto pos = [&](int32_t row, int32_t col) -> int32_t {
@@ -840,11 +891,13 @@ void Solver::setup_matrix(const HostMesh& hm, const Csr& c2c) {
         for (int32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) trans[k] = pos(cols[k], i);
     std::vector<int32_t> fpos(static_cast<std::size_t>(2) * hm.n_inner);
     for (int32_t f = 0; f < hm.n_inner; ++f) {
-        fpos[2 * f] = pos(hm.owner[f], hm.neigh[f]);
-        fpos[2 * f + 1] = pos(hm.neigh[f], hm.owner[f]);
+        fpos[2 * f] = pos(R(hm.owner[f]), R(hm.neigh[f]));
+        fpos[2 * f + 1] = pos(R(hm.neigh[f]), R(hm.owner[f]));
     }
     upload_or_throw(trans_, trans, stream_, "trans");
     upload_or_throw(face_pos_, fpos, stream_, "face_pos");
+    if (perm) upload_or_throw(row_of_, row_of_h_, stream_, "row_of");
+    dm_.row_of = perm ? row_of_.p : nullptr;
     alloc_or_throw(bjac_, static_cast<std::size_t>(std::max(hm.n_faces - hm.n_inner, 1)) * 25, "bjac");
     alloc_or_throw(b_, static_cast<std::size_t>(n) * nv_, "rhs");
     alloc_or_throw(du_, static_cast<std::size_t>(n) * nv_, "du");
@@ -1000,7 +1053,28 @@ void Solver::get_field(int field, double* out, int64_t count) {
         case CFDG_FIELD_JAC: {
             need = sys_->nnzb() * sys_->bs() * sys_->bs();
             if (count < need) throw Failure{CFDG_ERR_INVALID, "output buffer too small"};
-            sys_->get_values_host(out);
+            if (row_of_h_.empty()) {
+                sys_->get_values_host(out);
+                return;
+            }
+            // colour-ordered storage -> the reference's cell-ordered BSR
+            std::vector<double> tmp(static_cast<std::size_t>(need));
+            sys_->get_values_host(tmp.data());
+            const auto& rp = sys_->row_ptr_host();
+            const auto& cl = sys_->cols_host();
+            const int64_t b2 = int64_t(sys_->bs()) * sys_->bs();
+            std::vector<std::pair<int32_t, int32_t>> row;
+            int64_t w = 0;
+            for (int32_t c = 0; c < dm_.n; ++c) {
+                const int32_t r = row_of_h_[c];
+                row.clear();
+                for (int32_t k = rp[r]; k < rp[r + 1]; ++k) row.emplace_back(cell_of_h_[cl[k]], k);
+                std::sort(row.begin(), row.end());
+                for (const auto& e : row) {
+                    std::copy(tmp.begin() + e.second * b2, tmp.begin() + (e.second + 1) * b2, out + w * b2);
+                    ++w;
+                }
+            }
             return;
         }
         default: throw Failure{CFDG_ERR_INVALID, "unknown field id"};
@@ -1009,6 +1083,12 @@ void Solver::get_field(int field, double* out, int64_t count) {
     if (count < need) throw Failure{CFDG_ERR_INVALID, "output buffer too small"};
     cuda_check(cudaMemcpyAsync(out, src, sizeof(double) * need, cudaMemcpyDeviceToHost, stream_), "D2H");
     cuda_check(cudaStreamSynchronize(stream_), "sync");
+    if ((field == CFDG_FIELD_DU || field == CFDG_FIELD_RHS) && !row_of_h_.empty()) {
+        // linear-system vectors are stored in row (colour) order
+        std::vector<double> tmp(out, out + need);
+        for (int32_t c = 0; c < dm_.n; ++c)
+            for (int v = 0; v < nv_; ++v) out[int64_t(c) * nv_ + v] = tmp[int64_t(row_of_h_[c]) * nv_ + v];
+    }
 }
 
 void Solver::stage(int st) {
@@ -1151,7 +1231,7 @@ void Solver::prepare_guess_inputs() {
     ProfScope ps(&prof_, CFDG_KCAT_GUESS, stream_, 3,
                  double(dm_.n) * (nv_ * 8.0 * 4 + 16.0) +
                      double(dm_.n) * (kMlpIn * 2.0 + 8.0 * (nv_ * 3 + 2)) + double(c2c_.count) * 4.0);
-    launch_guess_scales(dm_.n, nv_, b_.p, dt_.p, vol_.p, du_prev_.p, gpart_.p, gscale_.p, stream_);
+    launch_guess_scales(dm_.n, dm_.row_of, nv_, b_.p, dt_.p, vol_.p, du_prev_.p, gpart_.p, gscale_.p, stream_);
     launch_guess_features(dm_, nv_, U_.p, b_.p, dt_.p, du_prev_.p, gscale_.p, cfl_now_, feat_.p, stream_);
     cuda_check(cudaGetLastError(), "guess launch");
 }
@@ -1196,7 +1276,7 @@ cfdg_step_result Solver::newton_step(double cfl) {
         const int64_t got = dataset_->reserve(want);
         if (got > 0) {
             ProfScope ps(&prof_, CFDG_KCAT_GUESS, stream_, 1, double(got) * (kMlpIn * 4.0 + nv_ * 8.0 + kMlpOut * 4.0));
-            launch_guess_append(dm_.n, nv_, ds_stride_, ds_phase_, got, feat_.p, du_.p, gscale_.p,
+            launch_guess_append(dm_.n, dm_.row_of, nv_, ds_stride_, ds_phase_, got, feat_.p, du_.p, gscale_.p,
                                 dataset_->X() + at * kMlpIn, dataset_->T() + at * kMlpOut, stream_);
         }
         ds_phase_ = (ds_phase_ + 1) % ds_stride_;

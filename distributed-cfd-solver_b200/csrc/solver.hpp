@@ -147,6 +147,7 @@ public:
     Profiler* profiler() { return prof_; }
     int check_every = 1;  // host polls the Krylov state every k iterations
 
+
 private:
     void build_ordering(int ordering);
     template <typename MT>
@@ -165,9 +166,11 @@ private:
     DevArray<int> err_;
     int ordering_ = -1, sweeps_ = 1;
     int last_guess_ = 0;
+
     double last_bnorm_ = 0.0;
     bool lu_ready_ = false;
     std::vector<int32_t> fwd_off_, bwd_off_;
+    std::vector<int32_t> fwd_first_, bwd_first_;  // first row of a contiguous group, -1 otherwise
     std::vector<double> fwd_bytes_[2], bwd_bytes_[2];  // algorithmic bytes of one pass, mode 0 / mode 1
     DevArray<int32_t> fwd_rows_, bwd_rows_;
     double spmv_bytes(int n_extra_vectors, bool read_y) const;
@@ -251,7 +254,8 @@ private:
     double* gnu_ = nullptr;
     // linear system
     std::unique_ptr<BsrSystem> sys_;
-    DevArray<int32_t> trans_, face_pos_;
+    DevArray<int32_t> trans_, face_pos_, row_of_;
+    std::vector<int32_t> row_of_h_, cell_of_h_;  // colour-ordered system: cell -> row, row -> cell
     DevArray<double> bjac_, b_, du_, norm_partials_, l2_;
     double* l2_host_ = nullptr;
     Profiler prof_;
