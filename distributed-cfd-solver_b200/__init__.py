@@ -152,6 +152,7 @@ _SIGS = {
     "cfdg_residual_norms": (C.c_int, [C.c_void_p, _dp]),
     "cfdg_run_steady": (C.c_int, [C.c_void_p, C.POINTER(RunResult)]),
     "cfdg_solver_freeze_limiter": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cfdg_solver_set_limiter": (C.c_int, [C.c_void_p, _dp, C.c_int64]),
     "cfdg_tc_selftest": (C.c_int, [C.c_int, C.c_int32, C.c_int32, _u16p, _u16p, _fp]),
     "cfdg_mlp_create": (C.c_int, [C.c_int, C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]),
     "cfdg_mlp_destroy": (C.c_int, [C.c_void_p]),
@@ -404,6 +405,11 @@ class Solver:
 
     def attach_dataset(self, ds: "Dataset | None", stride: int = 1):
         check(lib().cfdg_solver_attach_dataset(self._h, ds._h if ds is not None else None, stride))
+
+    def set_limiter(self, phi):
+        """Loads limiter values (5 x n) and freezes them."""
+        phi = np.ascontiguousarray(phi, dtype=np.float64).ravel()
+        check(lib().cfdg_solver_set_limiter(self._h, _dptr(phi), phi.size))
 
     def freeze_limiter(self, frozen: bool = True):
         check(lib().cfdg_solver_freeze_limiter(self._h, 1 if frozen else 0))

@@ -144,7 +144,9 @@ def sa_plate(scale: int = 1, seed: int = 2468, iterations: int = 200, mixed: boo
 
 
 def bump(scale: int = 1, seed: int = 777, iterations: int = 200, mixed: bool = True, mach: float = 0.85) -> Case:
-    """Transonic Euler bump, M=0.85, 160x80x80 hex -> 6 tets each (6,144,000 cells)."""
+    """Transonic Euler bump, M=0.85, 160x80x80 hex -> 6 tets each (6,144,000 cells).
+    CFL 1 -> 50 (at 100 the transient near the end of the ramp is marginal:
+    round-off differences decide whether it survives)."""
     nx, ny, nz = max(160 // scale, 6), max(80 // scale, 3), max(80 // scale, 3)
     T, p, M = 288.15, 101325.0, mach
     u = M * sound_speed(T)
@@ -153,7 +155,7 @@ def bump(scale: int = 1, seed: int = 777, iterations: int = 200, mixed: bool = T
     cfg = default_config(viscous=0, gradient=GRAD_LSQ_NODE, reconstruction=RECON_MUSCL, limiter=LIM_VENKATAKRISHNAN,
                          venkat_k=0.5, precond=PC_SGS, sgs_ordering=SGS_COLOR,
                          precision=1 if mixed else PREC_FP64,
-                         lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
+                         lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=50.0,
                          cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
                          limiter_freeze=LIMITER_FREEZE,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))

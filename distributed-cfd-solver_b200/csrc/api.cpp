@@ -262,6 +262,11 @@ int cfdg_solver_freeze_limiter(cfdg_solver* s, int32_t frozen) {
     CFDG_SOLVER_CALL(s, { s->impl->freeze_limiter(frozen != 0); });
 }
 
+int cfdg_solver_set_limiter(cfdg_solver* s, const double* phi_h, int64_t count) {
+    if (!phi_h) return CFDG_ERR_INVALID;
+    CFDG_SOLVER_CALL(s, s->impl->set_limiter(phi_h, count));
+}
+
 int cfdg_residual_norms(cfdg_solver* s, double* l2_h) {
     if (!l2_h) return CFDG_ERR_INVALID;
     CFDG_SOLVER_CALL(s, s->impl->residual_norms(l2_h));

@@ -68,13 +68,16 @@ struct JacStructure {
     const int32_t* trans;     // nnzb: position of the transposed block
     const int32_t* face_pos;  // 2*ni: block (owner,neigh), block (neigh,owner)
     bool full_viscous;        // thin-layer operator with the normal-stress term + no-slip ghost
+    // Spalart-Allmaras (6x6 blocks): per face d(nu_tilde flux)/d(rho nu_tilde)
+    // of owner [0, nf) and neighbour [nf, 2 nf), and the destruction
+    // derivative per cell; null without the model
+    const double* sa_jac;
+    const double* sa_dsrc;
 };
 template <typename MT>
 void launch_jacobian(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,
                      bool visc, MT* values, double* bface_scratch, cudaStream_t s);
-template <typename MT>
-void launch_sa_jacobian(const DevMesh& m, const DevFields& f, const JacStructure& js, const double* jac,
-                        const double* dsrc, MT* vals, cudaStream_t s);
+
 
 // ------------------------------------------------------------ linear algebra
 struct BsrView {

@@ -82,6 +82,8 @@ __global__ void __launch_bounds__(128) k_jac_offdiag(DevMesh m, DevFields f, Gas
     for (int r = 0; r < BS; ++r)
 #pragma unroll
         for (int c = 0; c < BS; ++c) stage[lane][r * BS + c] = (r < 5 && c < 5) ? to_mt<MT>(J[r * 5 + c]) : MT(0);
+    // nu_tilde entry of A(c0, c1): d F_nu / d (rho nu_tilde)_R (Picard: no coupling)
+    if (BS == 6) stage[lane][35] = to_mt<MT>(js.sa_jac[m.nf + fcs]);
     warp_store_blocks<MT, BS>(stage, js.face_pos[2 * fcs], valid, vals);
     // A(c1, c0) -= dF/dUL
     side_jacobian(g, UL, nx, ny, nz, half_area, diss, J);
@@ -90,6 +92,7 @@ __global__ void __launch_bounds__(128) k_jac_offdiag(DevMesh m, DevFields f, Gas
     for (int r = 0; r < BS; ++r)
 #pragma unroll
         for (int c = 0; c < BS; ++c) stage[lane][r * BS + c] = (r < 5 && c < 5) ? to_mt<MT>(-J[r * 5 + c]) : MT(0);
+    if (BS == 6) stage[lane][35] = to_mt<MT>(-js.sa_jac[fcs]);  // A(c1, c0) -= d F_nu / d (rho nu_tilde)_L
     warp_store_blocks<MT, BS>(stage, js.face_pos[2 * fcs + 1], valid, vals);
 }
 
@@ -129,30 +132,45 @@ __global__ void __launch_bounds__(128) k_jac_bface(DevMesh m, DevFields f, GasPa
 }
 
 // Diagonal block entry (c, e): -sum of transposed off-diagonal blocks of row
-// c, + boundary-face blocks, + alpha on the diagonal.  Entries outside the
-// 5x5 mean-flow part (bs = 6) are left to the turbulence assembly.
+// c, + boundary-face blocks, + alpha on the diagonal.  With 6x6 blocks the
+// nu_tilde row and column are zero except [5][5] = -sum of the transposed
+// [5][5] entries + the boundary faces' d F_nu / d (rho nu_tilde) + the
+// destruction derivative + alpha (Picard: no mean-flow coupling).
 template <typename MT, int BS>
 __global__ void __launch_bounds__(256) k_jac_diag(DevMesh m, const double* __restrict__ alpha, JacStructure js,
                                                   const double* __restrict__ bjac, MT* vals) {
+    constexpr int NE = BS * BS;
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= int64_t(m.n) * 25) return;
-    const int32_t c = static_cast<int32_t>(t / 25);
+    if (t >= int64_t(m.n) * NE) return;
+    const int32_t c = static_cast<int32_t>(t / NE);
     const int32_t row = row_index(m, c);
-    const int e = static_cast<int>(t % 25);
-    const int er = e / 5, ec = e % 5;
-    const int eb = er * BS + ec;
+    const int eb = static_cast<int>(t % NE);
+    const int er = eb / BS, ec = eb % BS;
     const int32_t d = js.diag[row];
     double v = 0.0;
-    for (int32_t k = js.row_ptr[row]; k < js.row_ptr[row + 1]; ++k) {
-        if (k == d) continue;
-        v -= static_cast<double>(vals[int64_t(js.trans[k]) * (BS * BS) + eb]);
+    if (er < 5 && ec < 5) {
+        const int e = er * 5 + ec;
+        for (int32_t k = js.row_ptr[row]; k < js.row_ptr[row + 1]; ++k) {
+            if (k == d) continue;
+            v -= static_cast<double>(vals[int64_t(js.trans[k]) * NE + eb]);
+        }
+        for (int32_t q = m.c2f_off[c]; q < m.c2f_off[c + 1]; ++q) {
+            const int32_t fc = m.c2f[q];
+            if (fc >= m.ni) v += bjac[int64_t(fc - m.ni) * 25 + e];
+        }
+        if (er == ec && alpha) v += alpha[c];
+    } else if (er == 5 && ec == 5) {
+        for (int32_t k = js.row_ptr[row]; k < js.row_ptr[row + 1]; ++k) {
+            if (k == d) continue;
+            v -= static_cast<double>(vals[int64_t(js.trans[k]) * NE + eb]);
+        }
+        for (int32_t q = m.c2f_off[c]; q < m.c2f_off[c + 1]; ++q) {
+            const int32_t fc = m.c2f[q];
+            if (fc >= m.ni) v += js.sa_jac[fc];
+        }
+        v += js.sa_dsrc[c] + alpha[c];
     }
-    for (int32_t q = m.c2f_off[c]; q < m.c2f_off[c + 1]; ++q) {
-        const int32_t fc = m.c2f[q];
-        if (fc >= m.ni) v += bjac[int64_t(fc - m.ni) * 25 + e];
-    }
-    if (er == ec && alpha) v += alpha[c];
-    vals[int64_t(d) * (BS * BS) + eb] = to_mt<MT>(v);
+    vals[int64_t(d) * NE + eb] = to_mt<MT>(v);
 }
 
 }  // namespace
@@ -175,9 +193,8 @@ static void launch_jacobian_t(const DevMesh& m, const DevFields& f, const GasPar
         if (visc) k_jac_bface<true, FULL><<<gr, 128, 0, s>>>(m, f, g, bface_scratch);
         else k_jac_bface<false, FULL><<<gr, 128, 0, s>>>(m, f, g, bface_scratch);
     }
-    const unsigned gd = grid_for(int64_t(m.n) * 25, 256);
-    if (bs == 5) k_jac_diag<MT, 5><<<gd, 256, 0, s>>>(m, f.alpha, js, bface_scratch, values);
-    else k_jac_diag<MT, 6><<<gd, 256, 0, s>>>(m, f.alpha, js, bface_scratch, values);
+    if (bs == 5) k_jac_diag<MT, 5><<<grid_for(int64_t(m.n) * 25, 256), 256, 0, s>>>(m, f.alpha, js, bface_scratch, values);
+    else k_jac_diag<MT, 6><<<grid_for(int64_t(m.n) * 36, 256), 256, 0, s>>>(m, f.alpha, js, bface_scratch, values);
 }
 
 template <typename MT>

@@ -317,6 +317,7 @@ void launch_gradient(const DevMesh& m, const double* src, double* dst, int nvars
     switch (nvars) {
         case 1: k_gradient<1><<<gr, 128, 0, s>>>(m, src, dst); break;
         case 5: k_gradient<5><<<gr, 128, 0, s>>>(m, src, dst); break;
+        case 6: k_gradient<6><<<gr, 128, 0, s>>>(m, src, dst); break;  // 5 primitives + nu_tilde
         default: break;
     }
 }

@@ -1,8 +1,8 @@
 // Spalart-Allmaras one-equation model on the device: ghost values and eddy
 // viscosity, the nu_tilde face sweep (upwind convection on the mean-flow
 // mass flux + skew-corrected diffusion), the cell gather with production /
-// destruction / cb2 sources, and the nu_tilde entries of the 6x6 Picard
-// Jacobian.  Follows include/cfd/solver/compressible/turbulence/
+// destruction / cb2 sources, and per face / cell the derivatives that the
+// Jacobian kernels place in the nu_tilde entries of the 6x6 Picard blocks.  Follows include/cfd/solver/compressible/turbulence/
 // spalart_allmaras.hpp (the reference module, which does not compile) with
 // the standard SA-1994 signs restored: the diffusive flux enters the
 // residual with a minus sign, the cb2 term is a source, S = sqrt(2 S_ij S_ij)
@@ -173,49 +173,6 @@ __global__ void __launch_bounds__(128) k_sa_cell(DevMesh m, DevFields f, SaParam
     dsrc[c] = m.vol[c] * 2.0 * sa.cw1 * fw * nu * id2;
 }
 
-// nu_tilde entries of the interior-face off-diagonal blocks: A(c0,c1)[5][5]
-// = dF/dU_R, A(c1,c0)[5][5] = -dF/dU_L (after the mean-flow blocks).
-template <typename MT>
-__global__ void k_sa_jac_offdiag(int32_t ni, int64_t nf, const int32_t* __restrict__ face_pos,
-                                 const double* __restrict__ jac, MT* vals) {
-    const int32_t fc = blockIdx.x * blockDim.x + threadIdx.x;
-    if (fc >= ni) return;
-    vals[int64_t(face_pos[2 * fc]) * 36 + 35] = static_cast<MT>(jac[nf + fc]);
-    vals[int64_t(face_pos[2 * fc + 1]) * 36 + 35] = static_cast<MT>(-jac[fc]);
-}
-
-// Row/column 5 of the diagonal blocks: zero coupling to the mean flow, and
-// [5][5] = -sum of transposed [5][5] entries + boundary-face entries +
-// (destruction derivative + alpha).
-template <typename MT>
-__global__ void k_sa_jac_diag(DevMesh m, const double* __restrict__ alpha, JacStructure js,
-                              const double* __restrict__ jac, const double* __restrict__ dsrc, MT* vals) {
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= int64_t(m.n) * 11) return;
-    const int32_t c = static_cast<int32_t>(t / 11);
-    const int32_t row = row_index(m, c);
-    const int e = static_cast<int>(t % 11);  // 0..4: [5][e], 5..9: [e-5][5], 10: [5][5]
-    MT* d = vals + int64_t(js.diag[row]) * 36;
-    if (e < 5) {
-        d[30 + e] = MT(0);
-    } else if (e < 10) {
-        d[(e - 5) * 6 + 5] = MT(0);
-    } else {
-        const int32_t dk = js.diag[row];
-        double v = 0.0;
-        for (int32_t k = js.row_ptr[row]; k < js.row_ptr[row + 1]; ++k) {
-            if (k == dk) continue;
-            v -= static_cast<double>(vals[int64_t(js.trans[k]) * 36 + 35]);
-        }
-        for (int32_t q = m.c2f_off[c]; q < m.c2f_off[c + 1]; ++q) {
-            const int32_t fc = m.c2f[q];
-            if (fc >= m.ni) v += jac[fc];
-        }
-        v += dsrc[c] + alpha[c];
-        d[35] = static_cast<MT>(v);
-    }
-}
-
 }  // namespace
 
 void launch_sa_pre(const DevMesh& m, const DevFields& f, const GasParams& g, const SaParams& sa, double* rhonu_g,
@@ -229,17 +186,5 @@ void launch_sa_sweep(const DevMesh& m, const DevFields& f, const GasParams& g, c
     k_sa_face<<<grid_for(m.nf, 128), 128, 0, s>>>(m, f, g, sa, rhonu_g, gnu, face, jac);
     k_sa_cell<<<grid_for(m.n, 128), 128, 0, s>>>(m, f, sa, face, gnu, dsrc);
 }
-
-template <typename MT>
-void launch_sa_jacobian(const DevMesh& m, const DevFields& f, const JacStructure& js, const double* jac,
-                        const double* dsrc, MT* vals, cudaStream_t s) {
-    if (m.ni > 0) k_sa_jac_offdiag<MT><<<grid_for(m.ni, 256), 256, 0, s>>>(m.ni, m.nf, js.face_pos, jac, vals);
-    k_sa_jac_diag<MT><<<grid_for(int64_t(m.n) * 11, 256), 256, 0, s>>>(m, f.alpha, js, jac, dsrc, vals);
-}
-
-template void launch_sa_jacobian<double>(const DevMesh&, const DevFields&, const JacStructure&, const double*,
-                                         const double*, double*, cudaStream_t);
-template void launch_sa_jacobian<float>(const DevMesh&, const DevFields&, const JacStructure&, const double*,
-                                        const double*, float*, cudaStream_t);
 
 }  // namespace cfdg

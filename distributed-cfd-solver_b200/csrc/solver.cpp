@@ -714,7 +714,7 @@ void Solver::setup_mesh(const cfdg_mesh_host& mesh) {
     // fields
     const std::size_t nt = static_cast<std::size_t>(dm_.nt), nn = static_cast<std::size_t>(n);
     alloc_or_throw(U_, nn * nv_, "U");
-    alloc_or_throw(q_, nt * 5, "q");
+    alloc_or_throw(q_, nt * (sa_ ? 6 : 5), "q");  // with SA, plane 5 holds nu_tilde
     alloc_or_throw(grad_, need_grad_ ? nt * 3 * nv_ : 1, "grad");
     alloc_or_throw(phi_, muscl_ ? nn * 5 : 1, "phi");
     alloc_or_throw(fflux_, static_cast<std::size_t>(nf) * 6, "fflux");
@@ -967,26 +967,24 @@ void Solver::setup_sa(const HostMesh& hm) {
     upload_or_throw(wall_dist_, wd, stream_, "wall distance");
     const std::size_t n = static_cast<std::size_t>(dm_.n), nt = static_cast<std::size_t>(dm_.nt);
     const std::size_t nf = static_cast<std::size_t>(dm_.nf), nb = static_cast<std::size_t>(std::max(dm_.nb, 1));
-    alloc_or_throw(nu_, nt, "nu_tilde");
     alloc_or_throw(rho_, nt, "rho");
     alloc_or_throw(mut_, nt, "mu_t");
     alloc_or_throw(rhonu_g_, nb, "ghost rho nu_tilde");
     alloc_or_throw(sa_face_, 2 * nf, "SA face");
     alloc_or_throw(sa_jac_, 2 * nf, "SA face jacobian");
     alloc_or_throw(sa_dsrc_, n, "SA destruction derivative");
-    for (DevArray<double>* a : {&nu_, &rho_, &mut_, &rhonu_g_, &sa_face_, &sa_jac_, &sa_dsrc_})
+    for (DevArray<double>* a : {&rho_, &mut_, &rhonu_g_, &sa_face_, &sa_jac_, &sa_dsrc_})
         cuda_check(cudaMemsetAsync(a->p, 0, a->count * sizeof(double), stream_), "memset");
     cuda_check(cudaStreamSynchronize(stream_), "setup sync");
     dm_.wall_dist = wall_dist_.p;
-    df_.nu = nu_.p;
+    df_.nu = q_.p + 5 * nt;  // the sixth plane of q: one gradient pass covers all six
     df_.rho = rho_.p;
     df_.mut = mut_.p;
     gnu_ = grad_.p + 15 * nt;  // nu_tilde gradient planes follow the 15 mean-flow planes
     ab_.sa_pre = n * (8.0 * 8 + 3 * 8.0) + double(dm_.nb) * (4 + 4 + 8 + 8 * 3 + 8 * 3);
-    ab_.sa_grad = n * 8.0 + double(g_col_.count) * (4 + 3 * 8.0) + n * 3 * 8.0;
+    ab_.sa_grad = n * 8.0 + n * 3 * 8.0;  // nu_tilde and its three planes (stencil counted with the mean flow)
     ab_.sa_face = double(nf) * (4 * 2 + 8 * 5 + 8 * 4 + 8 * 4) + double(dm_.nb) * (4 + 8) + nt * (8 * 2 + 8 * 3 + 8);
-    ab_.sa_jac = double(dm_.ni) * (4 * 2 + 8 * 2 + 2 * 4.0) + n * (4 * 3 + 8 * 2) + double(sys_->nnzb()) * (4 + 4) +
-                 double(sys_->nnzb()) * 11 * ((cfg_.precision == CFDG_PREC_MIXED) ? 4.0 : 8.0);
+    ab_.jac += double(nf) * 2 * 8.0 + n * 8.0;  // the face and destruction derivatives read by the 6x6 blocks
 }
 
 void Solver::sizes(int64_t* out) const {
@@ -1021,6 +1019,14 @@ void Solver::init_fields() {
     cuda_check(cudaStreamSynchronize(stream_), "init sync");
 }
 
+void Solver::set_limiter(const double* phi, int64_t count) {
+    if (!muscl_) throw Failure{CFDG_ERR_INVALID, "no limiter: the reconstruction is first order"};
+    if (count < int64_t(dm_.n) * 5) throw Failure{CFDG_ERR_INVALID, "limiter array smaller than 5 x n_cells"};
+    cuda_check(cudaMemcpyAsync(phi_.p, phi, sizeof(double) * 5 * dm_.n, cudaMemcpyHostToDevice, stream_), "H2D");
+    cuda_check(cudaStreamSynchronize(stream_), "sync");
+    limiter_frozen_ = true;
+}
+
 void Solver::set_state_host(const double* u, int64_t ld) {
     if (ld < dm_.n) throw Failure{CFDG_ERR_INVALID, "leading dimension smaller than n_cells"};
     have_prev_ = false;
@@ -1048,7 +1054,7 @@ void Solver::get_field(int field, double* out, int64_t count) {
         case CFDG_FIELD_RHS: src = b_.p; need = n * nv_; break;
         case CFDG_FIELD_MUT: src = mut_.p; need = sa_ ? nt : 0; break;
         case CFDG_FIELD_WALLDIST: src = wall_dist_.p; need = sa_ ? n : 0; break;
-        case CFDG_FIELD_NU: src = nu_.p; need = sa_ ? n : 0; break;
+        case CFDG_FIELD_NU: src = df_.nu; need = sa_ ? n : 0; break;
         case CFDG_FIELD_NU_GRAD: src = gnu_; need = sa_ ? nt * 3 : 0; break;
         case CFDG_FIELD_JAC: {
             need = sys_->nnzb() * sys_->bs() * sys_->bs();
@@ -1106,12 +1112,8 @@ void Solver::stage(int st) {
         }
         case CFDG_STAGE_GRADIENT:
             if (need_grad_) {
-                ProfScope ps(&prof_, CFDG_KCAT_GRADIENT, stream_, 1, ab_.grad);
-                launch_gradient(dm_, q_.p, grad_.p, 5, stream_);
-            }
-            if (sa_) {
-                ProfScope ps(&prof_, CFDG_KCAT_GRADIENT, stream_, 1, ab_.sa_grad);
-                launch_gradient(dm_, nu_.p, gnu_, 1, stream_);
+                ProfScope ps(&prof_, CFDG_KCAT_GRADIENT, stream_, 1, ab_.grad + (sa_ ? ab_.sa_grad : 0.0));
+                launch_gradient(dm_, q_.p, grad_.p, sa_ ? 6 : 5, stream_);
             }
             break;
         case CFDG_STAGE_LIMITER:
@@ -1165,19 +1167,14 @@ void Solver::assemble_jacobian() {
     js.trans = trans_.p;
     js.face_pos = face_pos_.p;
     js.full_viscous = cfg_.jacobian == CFDG_JAC_THIN_LAYER;
+    js.sa_jac = sa_ ? sa_jac_.p : nullptr;
+    js.sa_dsrc = sa_ ? sa_dsrc_.p : nullptr;
     {
         ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 3, ab_.jac);
         if (cfg_.precision == CFDG_PREC_MIXED)
             launch_jacobian<float>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values32(), bjac_.p, stream_);
         else
             launch_jacobian<double>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values64(), bjac_.p, stream_);
-    }
-    if (sa_) {
-        ProfScope ps(&prof_, CFDG_KCAT_TURBULENCE, stream_, 2, ab_.sa_jac);
-        if (cfg_.precision == CFDG_PREC_MIXED)
-            launch_sa_jacobian<float>(dm_, df_, js, sa_jac_.p, sa_dsrc_.p, sys_->values32(), stream_);
-        else
-            launch_sa_jacobian<double>(dm_, df_, js, sa_jac_.p, sa_dsrc_.p, sys_->values64(), stream_);
     }
     cuda_check(cudaGetLastError(), "jacobian launch");
 }

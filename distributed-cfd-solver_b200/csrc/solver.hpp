@@ -147,7 +147,6 @@ public:
     Profiler* profiler() { return prof_; }
     int check_every = 1;  // host polls the Krylov state every k iterations
 
-
 private:
     void build_ordering(int ordering);
     template <typename MT>
@@ -166,7 +165,6 @@ private:
     DevArray<int> err_;
     int ordering_ = -1, sweeps_ = 1;
     int last_guess_ = 0;
-
     double last_bnorm_ = 0.0;
     bool lu_ready_ = false;
     std::vector<int32_t> fwd_off_, bwd_off_;
@@ -210,6 +208,7 @@ public:
     void attach_guess(Mlp* m);
     void attach_dataset(Dataset* d, int32_t stride);
     void freeze_limiter(bool frozen) { limiter_frozen_ = frozen; }
+    void set_limiter(const double* phi, int64_t count);
 
 private:
     void setup_mesh(const cfdg_mesh_host& mesh);
@@ -247,10 +246,11 @@ private:
     std::vector<BcPatch> patches_h_;
     // fields
     DevArray<double> U_, q_, grad_, phi_, fflux_, res_, lam_, dt_, alpha_;
-    // Spalart-Allmaras: nu_tilde, rho, mu_t (n_total), ghost rho*nu_tilde (nb),
-    // face flux + spectral increments (2 nf), face d flux / d(rho nu_tilde) (2 nf),
-    // destruction derivative (n); the nu_tilde gradient lives in grad_ planes 15..17
-    DevArray<double> nu_, rho_, mut_, rhonu_g_, sa_face_, sa_jac_, sa_dsrc_;
+    // Spalart-Allmaras: rho, mu_t (n_total), ghost rho*nu_tilde (nb), face
+    // flux + spectral increments (2 nf), face d flux / d(rho nu_tilde) (2 nf),
+    // destruction derivative (n); nu_tilde is plane 5 of q_ and its gradient
+    // grad_ planes 15..17
+    DevArray<double> rho_, mut_, rhonu_g_, sa_face_, sa_jac_, sa_dsrc_;
     double* gnu_ = nullptr;
     // linear system
     std::unique_ptr<BsrSystem> sys_;
@@ -262,7 +262,7 @@ private:
     // algorithmic (unique-touch) bytes per launch of each residual-side kernel
     struct {
         double prim, grad, limiter, face_flux, cell_gather, jac, dt_rhs, state_update, norms;
-        double sa_pre, sa_grad, sa_face, sa_jac;
+        double sa_pre, sa_grad, sa_face;
     } ab_{};
     void compute_alg_bytes(int64_t n_grad_edges, int64_t n_c2c, int64_t n_c2f);
     cfdg_krylov_result last_krylov_{};

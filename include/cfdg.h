@@ -286,6 +286,10 @@ CFDG_API int cfdg_newton_step(cfdg_solver* s, double cfl, cfdg_step_result* out_
  * residual reuses the last computed phi (a smooth residual for the final
  * orders of convergence; not in the reference, which recomputes it). */
 CFDG_API int cfdg_solver_freeze_limiter(cfdg_solver* s, int32_t frozen);
+/* Loads limiter values (5 x n_cells, SoA as CFDG_FIELD_PHI) and freezes
+ * them: two runs given the same values converge to the same discrete
+ * solution. */
+CFDG_API int cfdg_solver_set_limiter(cfdg_solver* s, const double* phi_h, int64_t count);
 /* Solver::residual_norms (solver.hpp:740-756), nvars doubles. */
 CFDG_API int cfdg_residual_norms(cfdg_solver* s, double* l2_h);
 /* Allocation-free variant of cfdg_residual_norms, with no counterpart in the
