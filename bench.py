@@ -214,6 +214,22 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def max_over_ranks(ms: float, dist_mod, device: str) -> float:
+    """The slowest rank's time (all ranks take part; dist_mod None: one rank)."""
+    if dist_mod is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, cells: int, steps: int, t_max_ms: float) -> float:
+    """Whole-job Mcell-iter/s of `world` independent replicas of `cells`
+    cells that each ran `steps` iterations, timed by the slowest rank."""
+    return world * cells * steps / (t_max_ms * 1e-3) / 1e6
+
+
 def run_ours(args):
     world, rank, local = _dist()
     import torch
@@ -268,12 +284,8 @@ def run_ours(args):
     s.profile(False)
     kry_timed = list(kry)
     barrier()
-    t_max = ms
-    if pg is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * n * args.steps / (t_max * 1e-3) / 1e6
+    t_max = max_over_ranks(ms, pg, f"cuda:{local}")
+    value = replica_throughput(world, n, args.steps, t_max)
 
     # ---------------------------------------------------- end to end (C ABI)
     U_host = torch.empty(s.field_size(cb.FIELD_U), dtype=torch.float64, pin_memory=True)
@@ -293,11 +305,8 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if pg is not None:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * n * e2e_steps / (e2e_ms * 1e-3) / 1e6
+    e2e_ms = max_over_ranks(e2e_ms, pg, f"cuda:{local}")
+    e2e_value = replica_throughput(world, n, e2e_steps, e2e_ms)
     bytes_state = U_host.numel() * 8
 
     if rank == 0:
