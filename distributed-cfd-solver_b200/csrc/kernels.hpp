@@ -73,10 +73,11 @@ struct JacStructure {
     // derivative per cell; null without the model
     const double* sa_jac;
     const double* sa_dsrc;
+    const int32_t* cell_of;   // cell of each block row (colour-ordered system); null: row = cell
 };
 template <typename MT>
 void launch_jacobian(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,
-                     bool visc, MT* values, double* bface_scratch, cudaStream_t s);
+                     bool visc, MT* values, cudaStream_t s);
 
 
 // ------------------------------------------------------------ linear algebra

@@ -759,8 +759,11 @@ void Solver::compute_alg_bytes(int64_t E, int64_t n_c2c, int64_t n_c2f) {
     const double sa = (cfg_.precision == CFDG_PREC_MIXED) ? 4.0 : 8.0;
     const double b2 = double(nv_) * nv_;
     const double nnzb = sys_ ? double(sys_->nnzb()) : n + 2 * Fi;
-    ab_.jac = F * (2 * i4 + 4 * d + visc * d) + (n + nb) * 5 * d + n * d + Fi * 2 * i4 + nnzb * b2 * sa +
-              (nnzb - n) * b2 * sa + nnzb * i4 + (n + 1) * i4 + n * i4 + nb * 25 * d * 2 + double(n_c2f) * i4;
+    // row-centric assembly: face owner/neigh, normal, area (+ 1/|d|), primitives
+    // of cells and ghosts, alpha, CSR cell -> faces, face_pos, diagonal slots,
+    // boundary patch ids, the row -> cell map; every block written once
+    ab_.jac = F * (2 * i4 + 4 * d + visc * d) + (n + nb) * 5 * d + n * d + (n + 1) * i4 + double(n_c2f) * i4 +
+              Fi * 2 * i4 + n * i4 + nb * i4 + n * i4 + nnzb * b2 * sa;
     ab_.dt_rhs = n * (d * 2 + d * 2 + nv_ * d + 2 * nv_ * d);
     ab_.state_update = n * nv_ * d * 3;
     ab_.norms = n * nv_ * d;
@@ -896,9 +899,11 @@ void Solver::setup_matrix(const HostMesh& hm, const Csr& c2c) {
     }
     upload_or_throw(trans_, trans, stream_, "trans");
     upload_or_throw(face_pos_, fpos, stream_, "face_pos");
-    if (perm) upload_or_throw(row_of_, row_of_h_, stream_, "row_of");
+    if (perm) {
+        upload_or_throw(row_of_, row_of_h_, stream_, "row_of");
+        upload_or_throw(cell_of_, cell_of_h_, stream_, "cell_of");
+    }
     dm_.row_of = perm ? row_of_.p : nullptr;
-    alloc_or_throw(bjac_, static_cast<std::size_t>(std::max(hm.n_faces - hm.n_inner, 1)) * 25, "bjac");
     alloc_or_throw(b_, static_cast<std::size_t>(n) * nv_, "rhs");
     alloc_or_throw(du_, static_cast<std::size_t>(n) * nv_, "du");
     cuda_check(cudaMemsetAsync(du_.p, 0, du_.count * sizeof(double), stream_), "memset");
@@ -1169,12 +1174,13 @@ void Solver::assemble_jacobian() {
     js.full_viscous = cfg_.jacobian == CFDG_JAC_THIN_LAYER;
     js.sa_jac = sa_ ? sa_jac_.p : nullptr;
     js.sa_dsrc = sa_ ? sa_dsrc_.p : nullptr;
+    js.cell_of = row_of_h_.empty() ? nullptr : cell_of_.p;
     {
-        ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 3, ab_.jac);
+        ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 1, ab_.jac);
         if (cfg_.precision == CFDG_PREC_MIXED)
-            launch_jacobian<float>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values32(), bjac_.p, stream_);
+            launch_jacobian<float>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values32(), stream_);
         else
-            launch_jacobian<double>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values64(), bjac_.p, stream_);
+            launch_jacobian<double>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values64(), stream_);
     }
     cuda_check(cudaGetLastError(), "jacobian launch");
 }

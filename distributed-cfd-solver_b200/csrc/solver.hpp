@@ -254,9 +254,9 @@ private:
     double* gnu_ = nullptr;
     // linear system
     std::unique_ptr<BsrSystem> sys_;
-    DevArray<int32_t> trans_, face_pos_, row_of_;
+    DevArray<int32_t> trans_, face_pos_, row_of_, cell_of_;
     std::vector<int32_t> row_of_h_, cell_of_h_;  // colour-ordered system: cell -> row, row -> cell
-    DevArray<double> bjac_, b_, du_, norm_partials_, l2_;
+    DevArray<double> b_, du_, norm_partials_, l2_;
     double* l2_host_ = nullptr;
     Profiler prof_;
     // algorithmic (unique-touch) bytes per launch of each residual-side kernel
