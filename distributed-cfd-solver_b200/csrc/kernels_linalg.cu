@@ -68,15 +68,34 @@ __global__ void __launch_bounds__(256) k_spmv(BsrView A, const MT* __restrict__ 
 }
 
 // -------------------------------------------------------- block LU setup
+// One thread per block row; the CTA's 128 diagonal blocks are staged through
+// shared memory so that the loads (one block per 25 / 36 consecutive
+// threads) and the stores (the CTA's LU blocks are one contiguous range) are
+// coalesced.
+constexpr int kLuThreads = 128;
+
 template <typename MT, int BS>
-__global__ void k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu, int8_t* __restrict__ piv,
-                     int* __restrict__ err) {
-    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
+__global__ void __launch_bounds__(kLuThreads) k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu,
+                                                   int8_t* __restrict__ piv, int* __restrict__ err) {
+    constexpr int B2 = BS * BS;
+    __shared__ MT sm[kLuThreads * B2];
+    const int32_t r0 = blockIdx.x * kLuThreads;
+    const int32_t nrows = min(kLuThreads, A.n - r0);
+    for (int q = threadIdx.x; q < nrows * B2; q += kLuThreads) {
+        const int row = q / B2, e = q - row * B2;
+        sm[q] = vals[int64_t(A.diag[r0 + row]) * B2 + e];
+    }
+    __syncthreads();
+    const int32_t i = r0 + threadIdx.x;
+    const bool act = threadIdx.x < nrows;
     double a[BS * BS];
-    const MT* src = vals + int64_t(A.diag[i]) * (BS * BS);
+    if (act) {
 #pragma unroll
-    for (int e = 0; e < BS * BS; ++e) a[e] = static_cast<double>(src[e]);
+        for (int e = 0; e < BS * BS; ++e) a[e] = static_cast<double>(sm[threadIdx.x * B2 + e]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < BS * BS; ++e) a[e] = (e % (BS + 1) == 0) ? 1.0 : 0.0;
+    }
     int8_t pv[BS];
     bool ok = true;
 #pragma unroll
@@ -114,20 +133,25 @@ __global__ void k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu
             for (int j = k + 1; j < BS; ++j) a[r * BS + j] -= l * a[k * BS + j];
         }
     }
-    MT* dst = lu + int64_t(i) * (BS * BS);
+    __syncthreads();  // every thread has read its block
+    if (act) {
 #pragma unroll
-    for (int e = 0; e < BS * BS; ++e) dst[e] = static_cast<MT>(a[e]);
+        for (int e = 0; e < BS * BS; ++e) sm[threadIdx.x * B2 + e] = static_cast<MT>(a[e]);
 #pragma unroll
-    for (int k = 0; k < BS; ++k) piv[int64_t(i) * BS + k] = pv[k];
-    // +(i+1): zero pivot (singular block); -(i+1): non-finite entries
-    bool finite = true;
+        for (int k = 0; k < BS; ++k) piv[int64_t(i) * BS + k] = pv[k];
+        // +(i+1): zero pivot (singular block); -(i+1): non-finite entries
+        bool finite = true;
 #pragma unroll
-    for (int e = 0; e < BS * BS; ++e) finite = finite && isfinite(a[e]);
-    if (!ok) {
-        atomicCAS(err, 0, i + 1);
-    } else if (!finite) {
-        atomicCAS(err, 0, -(i + 1));
+        for (int e = 0; e < BS * BS; ++e) finite = finite && isfinite(a[e]);
+        if (!ok) {
+            atomicCAS(err, 0, i + 1);
+        } else if (!finite) {
+            atomicCAS(err, 0, -(i + 1));
+        }
     }
+    __syncthreads();
+    MT* dst = lu + int64_t(r0) * B2;
+    for (int q = threadIdx.x; q < nrows * B2; q += kLuThreads) dst[q] = sm[q];
 }
 
 // Pivoted forward/backward substitution of one block (lu_solve_block) in
@@ -458,13 +482,13 @@ void launch_spmv_ex(const BsrView& A, const MT* vals, const double* x, double* y
 
 template <typename MT>
 void launch_lu_setup(const BsrView& A, const MT* vals, MT* lu, int8_t* piv, int* err_flag, cudaStream_t s) {
-    const unsigned gr = grid_for(A.n, 128);
+    const unsigned gr = grid_for(A.n, kLuThreads);
     switch (A.bs) {
-        case 1: k_lu<MT, 1><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
-        case 3: k_lu<MT, 3><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
-        case 4: k_lu<MT, 4><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
-        case 5: k_lu<MT, 5><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
-        case 6: k_lu<MT, 6><<<gr, 128, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 1: k_lu<MT, 1><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 3: k_lu<MT, 3><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 4: k_lu<MT, 4><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 5: k_lu<MT, 5><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 6: k_lu<MT, 6><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
         default: break;
     }
 }

@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(128) k_gradient(DevMesh m, const double* __res
         gz[v] = 0.0;
     }
     const int32_t j1 = m.g_off[c + 1];
+#pragma unroll 4
     for (int32_t j = m.g_off[c]; j < j1; ++j) {
         const int32_t nb = m.g_col[j];
         const double wx = m.g_wx[j], wy = m.g_wy[j], wz = m.g_wz[j];
