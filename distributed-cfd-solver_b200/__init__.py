@@ -45,6 +45,7 @@ KRYLOV_CONVERGED, KRYLOV_DIVERGED, KRYLOV_MAX_ITERATIONS = 0, 1, 2
 (FIELD_U, FIELD_Q, FIELD_GRAD, FIELD_PHI, FIELD_RES, FIELD_LAM, FIELD_DT, FIELD_ALPHA, FIELD_JAC, FIELD_DU,
  FIELD_MUT, FIELD_WALLDIST, FIELD_RHS, FIELD_NU, FIELD_NU_GRAD) = range(15)
 JAC_REFERENCE, JAC_THIN_LAYER = 0, 1
+KRYLOV_DEVICE_LOOP, KRYLOV_HOST_LOOP = 0, 1
 STAGE_PRIMITIVES, STAGE_GRADIENT, STAGE_LIMITER, STAGE_FLUXES = range(4)
 KCAT_NAMES = ("primitives", "gradient", "limiter", "face_flux", "cell_gather", "jacobian", "lu", "spmv", "sgs",
               "krylov", "update", "turbulence", "guess")
@@ -82,7 +83,7 @@ class Config(C.Structure):
                 ("precond", C.c_int32), ("sgs_ordering", C.c_int32), ("sgs_sweeps", C.c_int32),
                 ("lin_max_iterations", C.c_int32), ("cfl_ramp_iterations", C.c_int32),
                 ("residual_interval", C.c_int32), ("convergence_monitor", C.c_int32), ("jacobian", C.c_int32),
-                ("limiter_freeze", C.c_int32), ("reserved_", C.c_int32),
+                ("limiter_freeze", C.c_int32), ("krylov_loop", C.c_int32),
                 ("gamma", C.c_double), ("gas_constant", C.c_double), ("prandtl", C.c_double),
                 ("prandtl_turb", C.c_double), ("init_rho", C.c_double), ("init_p", C.c_double),
                 ("init_velocity", C.c_double * 3), ("venkat_k", C.c_double), ("cfl", C.c_double),

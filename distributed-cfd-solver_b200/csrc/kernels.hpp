@@ -65,7 +65,6 @@ struct JacStructure {
     const int32_t* row_ptr;   // n+1
     const int32_t* cols;      // nnzb
     const int32_t* diag;      // n
-    const int32_t* trans;     // nnzb: position of the transposed block
     const int32_t* face_pos;  // 2*ni: block (owner,neigh), block (neigh,owner)
     bool full_viscous;        // thin-layer operator with the normal-stress term + no-slip ghost
     // Spalart-Allmaras (6x6 blocks): per face d(nu_tilde flux)/d(rho nu_tilde)

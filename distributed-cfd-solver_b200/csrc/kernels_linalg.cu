@@ -21,18 +21,35 @@ template <typename MT>
 __device__ __forceinline__ double ld(const MT* p) { return static_cast<double>(__ldg(p)); }
 
 // --------------------------------------------------------------- SpMV
+// Vector kernels and the SpMV run a fixed grid of at most kVecGridCap
+// blocks (8 resident 256-thread blocks on each of 148 SMs) striding over
+// the vector, so that the per-block partial sums of the fused inner
+// products number at most kVecGridCap and the single-block finalisers read
+// them in a few loads per thread.  The grid depends only on the length, so
+// the summation order, and the result, is the same run to run.
+constexpr int kVecThreads = 256;
+constexpr int64_t kVecGridCap = 148 * 8;
+
+inline unsigned vec_grid(int64_t len) {
+    const int64_t g = grid_for(len, kVecThreads);
+    return static_cast<unsigned>(g < kVecGridCap ? g : kVecGridCap);
+}
+
 // One thread per (block row, component): y_i[ii] = alpha * sum_k sum_jj
 // A_k[ii][jj] x_col(k)[jj] + beta * y.  Optional fused dot products of y
 // (or other vectors) for the Krylov scalars, reduced per block.
 template <typename MT, int BS, int ND>
-__global__ void __launch_bounds__(256) k_spmv(BsrView A, const MT* __restrict__ vals, const double* __restrict__ x,
-                                              double* __restrict__ y, double alpha, double beta, DotSpec ds,
-                                              double* __restrict__ partials, const int* __restrict__ active) {
+__global__ void __launch_bounds__(kVecThreads) k_spmv(BsrView A, const MT* __restrict__ vals,
+                                                      const double* __restrict__ x, double* __restrict__ y,
+                                                      double alpha, double beta, DotSpec ds,
+                                                      double* __restrict__ partials, const int* __restrict__ active) {
     if (active && *active != 0) return;
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t N = int64_t(A.n) * BS;
-    double yv = 0.0;
-    if (t < N) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    double pr[ND > 0 ? ND : 1];
+#pragma unroll
+    for (int k = 0; k < (ND > 0 ? ND : 1); ++k) pr[k] = 0.0;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < N; t += stride) {
         const int32_t row = static_cast<int32_t>(t / BS);
         const int ii = static_cast<int>(t % BS);
         double acc = 0.0;
@@ -45,26 +62,22 @@ __global__ void __launch_bounds__(256) k_spmv(BsrView A, const MT* __restrict__ 
             for (int jj = 0; jj < BS; ++jj) s += ld(a + jj) * xb[jj];
             acc += s;
         }
+        double yv;
         if (alpha == 1.0 && beta == 0.0) yv = acc;
         else if (beta == 1.0) yv = y[t] + alpha * acc;
         else if (beta == 0.0) yv = alpha * acc;
         else yv = alpha * acc + beta * y[t];
         y[t] = yv;
-    }
-    if constexpr (ND > 0) {
-        double pr[ND];
+        if constexpr (ND > 0) {
 #pragma unroll
-        for (int k = 0; k < ND; ++k) {
-            if (t < N) {
+            for (int k = 0; k < ND; ++k) {
                 const double a = ds.a[k] ? ds.a[k][t] : yv;
                 const double b = ds.b[k] ? ds.b[k][t] : yv;
-                pr[k] = a * b;
-            } else {
-                pr[k] = 0.0;
+                pr[k] += a * b;
             }
         }
-        block_reduce_store<ND, 256>(pr, partials + size_t(blockIdx.x) * ND);
     }
+    if constexpr (ND > 0) block_reduce_store<ND, kVecThreads>(pr, partials + size_t(blockIdx.x) * ND);
 }
 
 // -------------------------------------------------------- block LU setup
@@ -193,6 +206,14 @@ __device__ __forceinline__ void lu_solve(const MT* __restrict__ lu, const int8_t
 // ascending order, as the sequential sweep), the group exchanges s by warp
 // shuffles, and each lane solves the pivoted LU system and keeps its entry.
 // MODE 1 skips the neighbour sum (all neighbour z are still zero).
+// MODE 2 and 3 are the two halves of the first symmetric sweep of a
+// colour-ordered matrix (every colour a contiguous row range, colours
+// ascending, so "column < row" means "earlier colour"):
+//   MODE 2 (forward)  y_i = D_i^-1 (r_i - sum_{k < diag} A_ik y_k);
+//   MODE 3 (backward) z_i = y_i - D_i^-1 sum_{k > diag} A_ik z_k,
+// which equals the full-row backward update D_i^-1 (r_i - sum_lower A y -
+// sum_upper A z) because (D + L) y = r, and reads neither r nor the lower
+// blocks.
 template <typename MT, int BS, int MODE>
 __global__ void __launch_bounds__(256) k_sgs_rows(BsrView A, const MT* __restrict__ vals, const MT* __restrict__ lu,
                                                   const int8_t* __restrict__ piv, const int32_t* __restrict__ rows,
@@ -209,12 +230,13 @@ __global__ void __launch_bounds__(256) k_sgs_rows(BsrView A, const MT* __restric
     double s = 0.0;
     if (act) {
         i = rows ? rows[slot] : row0 + static_cast<int32_t>(slot);  // null: a contiguous group
-        s = r[int64_t(i) * BS + ii];
-        if (MODE == 0) {
+        s = (MODE == 3) ? 0.0 : r[int64_t(i) * BS + ii];
+        if (MODE != 1) {
             const int32_t d = A.diag[i];
-            const int32_t k1 = A.row_ptr[i + 1];
-            for (int32_t k = A.row_ptr[i]; k < k1; ++k) {
-                if (k == d) continue;
+            const int32_t k0 = (MODE == 3) ? d + 1 : A.row_ptr[i];
+            const int32_t k1 = (MODE == 2) ? d : A.row_ptr[i + 1];
+            for (int32_t k = k0; k < k1; ++k) {
+                if (MODE == 0 && k == d) continue;
                 const MT* a = vals + int64_t(k) * (BS * BS) + ii * BS;
                 const double* zb = z + int64_t(A.cols[k]) * BS;
                 double t = 0.0;
@@ -234,36 +256,30 @@ __global__ void __launch_bounds__(256) k_sgs_rows(BsrView A, const MT* __restric
 #pragma unroll
         for (int j = 1; j < BS; ++j)
             if (j == ii) out = b[j];
+        // MODE 3: b solved D x = -sum_upper A z, so z_i = y_i + x
+        if (MODE == 3) out = z[int64_t(i) * BS + ii] + out;
         z[int64_t(i) * BS + ii] = out;
     }
 }
 
 // ------------------------------------------------------ Krylov kernels
-__global__ void __launch_bounds__(256) k_dot_partials(int64_t len, DotSpec ds, int nd, double* __restrict__ partials) {
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    double pr[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (t < len) {
-        for (int k = 0; k < nd; ++k) pr[k] = ds.a[k][t] * ds.b[k][t];
-    }
-    block_reduce_store<5, 256>(pr, partials + size_t(blockIdx.x) * 5);
-}
-
 // r = b - v, r0 = r, p = r; partial sums of |b|^2 and |r|^2.
-__global__ void __launch_bounds__(256) k_krylov_init(int64_t len, const double* __restrict__ b, const double* __restrict__ v,
-                                                     double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
-                                                     double* __restrict__ partials) {
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kVecThreads) k_krylov_init(int64_t len, const double* __restrict__ b,
+                                                             const double* __restrict__ v, double* __restrict__ r,
+                                                             double* __restrict__ r0, double* __restrict__ p,
+                                                             double* __restrict__ partials) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     double pr[2] = {0.0, 0.0};
-    if (t < len) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < len; t += stride) {
         const double bt = b[t];
         const double rt = bt + (-1.0) * v[t];
         r[t] = rt;
         r0[t] = rt;
         p[t] = rt;
-        pr[0] = bt * bt;
-        pr[1] = rt * rt;
+        pr[0] += bt * bt;
+        pr[1] += rt * rt;
     }
-    block_reduce_store<2, 256>(pr, partials + size_t(blockIdx.x) * 2);
+    block_reduce_store<2, kVecThreads>(pr, partials + size_t(blockIdx.x) * 2);
 }
 
 // Sum of column k of the per-block partials (stride values per block) by the
@@ -351,12 +367,14 @@ __global__ void k_krylov_begin(KrylovScalars* ks) {
 }
 
 // s = r - alpha v
-__global__ void __launch_bounds__(256) k_krylov_s(int64_t len, const KrylovScalars* __restrict__ ks, const double* __restrict__ r,
-                                                  const double* __restrict__ v, double* __restrict__ s) {
+__global__ void __launch_bounds__(kVecThreads) k_krylov_s(int64_t len, const KrylovScalars* __restrict__ ks,
+                                                          const double* __restrict__ r, const double* __restrict__ v,
+                                                          double* __restrict__ s) {
     if (ks->state != KS_RUNNING) return;
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= len) return;
-    s[t] = r[t] + (-ks->alpha) * v[t];
+    const double alpha = ks->alpha;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < len; t += stride)
+        s[t] = r[t] + (-alpha) * v[t];
 }
 
 // Five fused inner products -> omega, reconstructed |r|, rho_next
@@ -383,17 +401,18 @@ __global__ void k_krylov_omega(KrylovScalars* ks, const double* __restrict__ par
 
 // x += alpha phat + omega shat; r = s - omega t; next p = r + beta (p - omega v);
 // partial |r|^2 for the periodic true-norm refresh.
-__global__ void __launch_bounds__(256) k_krylov_update(int64_t len, const KrylovScalars* __restrict__ ks,
-                                                       double* __restrict__ x, const double* __restrict__ phat,
-                                                       const double* __restrict__ shat, const double* __restrict__ s,
-                                                       const double* __restrict__ tv, double* __restrict__ r,
-                                                       double* __restrict__ p, const double* __restrict__ v,
-                                                       double* __restrict__ partials) {
-    const bool run = ks->state == KS_RUNNING;
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kVecThreads) k_krylov_update(int64_t len, const KrylovScalars* __restrict__ ks,
+                                                               double* __restrict__ x, const double* __restrict__ phat,
+                                                               const double* __restrict__ shat,
+                                                               const double* __restrict__ s,
+                                                               const double* __restrict__ tv, double* __restrict__ r,
+                                                               double* __restrict__ p, const double* __restrict__ v,
+                                                               double* __restrict__ partials) {
+    if (ks->state != KS_RUNNING) return;  // uniform across the grid
+    const double alpha = ks->alpha, omega = ks->omega_new, beta = ks->beta;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     double pr[1] = {0.0};
-    if (run && t < len) {
-        const double alpha = ks->alpha, omega = ks->omega_new, beta = ks->beta;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < len; t += stride) {
         double xv = x[t] + alpha * phat[t];
         xv = xv + omega * shat[t];
         x[t] = xv;
@@ -403,10 +422,9 @@ __global__ void __launch_bounds__(256) k_krylov_update(int64_t len, const Krylov
         pv = pv + (-beta * omega) * v[t];
         pv = pv + 1.0 * rv;
         p[t] = pv;
-        pr[0] = rv * rv;
+        pr[0] += rv * rv;
     }
-    if (!run) return;  // uniform across the grid
-    block_reduce_store<1, 256>(pr, partials + size_t(blockIdx.x));
+    block_reduce_store<1, kVecThreads>(pr, partials + size_t(blockIdx.x));
 }
 
 // Post-update checks, refresh every 32 iterations, convergence test
@@ -439,23 +457,28 @@ __global__ void k_krylov_post(KrylovScalars* ks, const double* __restrict__ part
     ks->omega = omega_new;
 }
 
-__global__ void k_copy(int64_t len, const double* __restrict__ a, double* __restrict__ b, const int* active) {
-    if (active && *active != 0) return;
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t < len) b[t] = a[t];
+// The while-condition of the device loop.  body_runs grows by one per body
+// run whatever the state, so the loop ends after at most max_it runs even if
+// the state were never updated.
+__global__ void k_krylov_cond(KrylovScalars* ks, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0) return;
+    const int runs = ks->body_runs + 1;
+    ks->body_runs = runs;
+    const bool more = ks->state == KS_RUNNING && runs < ks->max_it;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
 }  // namespace
 
 // ------------------------------------------------------------- launchers
-int spmv_blocks(int32_t n, int32_t bs) { return static_cast<int>(grid_for(int64_t(n) * bs, 256)); }
+int spmv_blocks(int32_t n, int32_t bs) { return static_cast<int>(vec_grid(int64_t(n) * bs)); }
 
 template <typename MT>
 void launch_spmv_ex(const BsrView& A, const MT* vals, const double* x, double* y, double alpha, double beta,
                     const DotSpec& ds, double* partials, const int* active, cudaStream_t s) {
-    const unsigned gr = grid_for(int64_t(A.n) * A.bs, 256);
+    const unsigned gr = vec_grid(int64_t(A.n) * A.bs);
     const int nd = ds.n;
-#define CFDG_SPMV(BS, ND) k_spmv<MT, BS, ND><<<gr, 256, 0, s>>>(A, vals, x, y, alpha, beta, ds, partials, active)
+#define CFDG_SPMV(BS, ND) k_spmv<MT, BS, ND><<<gr, kVecThreads, 0, s>>>(A, vals, x, y, alpha, beta, ds, partials, active)
     if (A.bs == 5) {
         if (nd == 0) CFDG_SPMV(5, 0);
         else if (nd == 1) CFDG_SPMV(5, 1);
@@ -501,9 +524,11 @@ void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const in
     const int gpw = 32 / A.bs;
     const int64_t warps = (int64_t(n_rows) + gpw - 1) / gpw;
     const unsigned gr = grid_for(warps * 32, 256);
-#define CFDG_SGS(BS)                                                                                          \
-    if (mode == 0) k_sgs_rows<MT, BS, 0><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active); \
-    else k_sgs_rows<MT, BS, 1><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active)
+#define CFDG_SGS(BS)                                                                                            \
+    if (mode == 0) k_sgs_rows<MT, BS, 0><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active);   \
+    else if (mode == 1) k_sgs_rows<MT, BS, 1><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active); \
+    else if (mode == 2) k_sgs_rows<MT, BS, 2><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active); \
+    else k_sgs_rows<MT, BS, 3><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active)
     switch (A.bs) {
         case 1: CFDG_SGS(1); break;
         case 3: CFDG_SGS(3); break;
@@ -515,39 +540,32 @@ void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const in
 #undef CFDG_SGS
 }
 
-int dot_blocks(int64_t len) { return static_cast<int>(grid_for(len, 256)); }
-
-void launch_dots(int64_t len, const DotSpec& ds, double* partials, cudaStream_t s) {
-    k_dot_partials<<<grid_for(len, 256), 256, 0, s>>>(len, ds, ds.n, partials);
-}
-
-void launch_copy(int64_t len, const double* a, double* b, const int* active, cudaStream_t s) {
-    k_copy<<<grid_for(len, 256), 256, 0, s>>>(len, a, b, active);
-}
+int dot_blocks(int64_t len) { return static_cast<int>(vec_grid(len)); }
 
 void launch_krylov_init(int64_t len, const double* b, const double* v, double* r, double* r0, double* p,
                         double* partials, KrylovScalars* ks, cudaStream_t s) {
-    const unsigned gr = grid_for(len, 256);
-    k_krylov_init<<<gr, 256, 0, s>>>(len, b, v, r, r0, p, partials);
+    const unsigned gr = vec_grid(len);
+    k_krylov_init<<<gr, kVecThreads, 0, s>>>(len, b, v, r, r0, p, partials);
     k_krylov_init_fin<<<1, kFinThreads, 0, s>>>(ks, partials, static_cast<int>(gr));
 }
-__global__ void __launch_bounds__(256) k_krylov_guess_reset(int64_t len, const KrylovScalars* __restrict__ ks,
-                                                            const double* __restrict__ b, double* __restrict__ x,
-                                                            double* __restrict__ r, double* __restrict__ r0,
-                                                            double* __restrict__ p) {
+__global__ void __launch_bounds__(kVecThreads) k_krylov_guess_reset(int64_t len, const KrylovScalars* __restrict__ ks,
+                                                                    const double* __restrict__ b, double* __restrict__ x,
+                                                                    double* __restrict__ r, double* __restrict__ r0,
+                                                                    double* __restrict__ p) {
     if (ks->guess != 2) return;  // uniform
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= len) return;
-    const double bt = b[t];
-    x[t] = 0.0;
-    r[t] = bt;
-    r0[t] = bt;
-    p[t] = bt;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < len; t += stride) {
+        const double bt = b[t];
+        x[t] = 0.0;
+        r[t] = bt;
+        r0[t] = bt;
+        p[t] = bt;
+    }
 }
 
 void launch_krylov_guess_reset(int64_t len, const KrylovScalars* ks, const double* b, double* x, double* r, double* r0,
                                double* p, cudaStream_t s) {
-    k_krylov_guess_reset<<<grid_for(len, 256), 256, 0, s>>>(len, ks, b, x, r, r0, p);
+    k_krylov_guess_reset<<<vec_grid(len), kVecThreads, 0, s>>>(len, ks, b, x, r, r0, p);
 }
 
 void launch_krylov_begin(KrylovScalars* ks, cudaStream_t s) { k_krylov_begin<<<1, 32, 0, s>>>(ks); }
@@ -556,7 +574,7 @@ void launch_krylov_gamma(KrylovScalars* ks, const double* partials, int nblocks,
 }
 void launch_krylov_s(int64_t len, const KrylovScalars* ks, const double* r, const double* v, double* sv,
                      cudaStream_t s) {
-    k_krylov_s<<<grid_for(len, 256), 256, 0, s>>>(len, ks, r, v, sv);
+    k_krylov_s<<<vec_grid(len), kVecThreads, 0, s>>>(len, ks, r, v, sv);
 }
 void launch_krylov_omega(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s) {
     k_krylov_omega<<<1, kFinThreads, 0, s>>>(ks, partials, nblocks);
@@ -564,7 +582,7 @@ void launch_krylov_omega(KrylovScalars* ks, const double* partials, int nblocks,
 void launch_krylov_update(int64_t len, const KrylovScalars* ks, double* x, const double* phat, const double* shat,
                           const double* sv, const double* tv, double* r, double* p, const double* v,
                           double* partials, cudaStream_t s) {
-    k_krylov_update<<<grid_for(len, 256), 256, 0, s>>>(len, ks, x, phat, shat, sv, tv, r, p, v, partials);
+    k_krylov_update<<<vec_grid(len), kVecThreads, 0, s>>>(len, ks, x, phat, shat, sv, tv, r, p, v, partials);
 }
 void launch_krylov_post(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s) {
     k_krylov_post<<<1, kFinThreads, 0, s>>>(ks, partials, nblocks);
@@ -580,5 +598,9 @@ template void launch_sgs_rows_ex<double>(const BsrView&, const double*, const do
                                          int32_t, int32_t, const double*, double*, int, const int*, cudaStream_t);
 template void launch_sgs_rows_ex<float>(const BsrView&, const float*, const float*, const int8_t*, const int32_t*,
                                         int32_t, int32_t, const double*, double*, int, const int*, cudaStream_t);
+
+void launch_krylov_cond(KrylovScalars* ks, cudaGraphConditionalHandle h, cudaStream_t s) {
+    k_krylov_cond<<<1, 32, 0, s>>>(ks, h);
+}
 
 }  // namespace cfdg

@@ -18,6 +18,7 @@ struct KrylovScalars {
     int it;
     int max_it;
     int guess;  // in: 1 when x holds an initial guess that may be rejected; out: 2 when rejected
+    int body_runs;  // device loop: iterations the graph body has run (bounds the loop by max_it)
     double rel_tol, abs_tol;
     double bnorm, scale, tol, initial, rnorm;
     double rho, rho_old, rho_new, alpha, omega, omega_new, beta;
@@ -38,8 +39,6 @@ template <typename MT>
 void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* rows,
                         int32_t row0, int32_t n_rows, const double* r, double* z, int mode, const int* active,
                         cudaStream_t s);
-void launch_dots(int64_t len, const DotSpec& ds, double* partials, cudaStream_t s);
-void launch_copy(int64_t len, const double* a, double* b, const int* active, cudaStream_t s);
 void launch_krylov_init(int64_t len, const double* b, const double* v, double* r, double* r0, double* p,
                         double* partials, KrylovScalars* ks, cudaStream_t s);
 // After launch_krylov_init: a rejected initial guess (||b - A x0|| >=
@@ -55,5 +54,8 @@ void launch_krylov_update(int64_t len, const KrylovScalars* ks, double* x, const
                           const double* sv, const double* tv, double* r, double* p, const double* v,
                           double* partials, cudaStream_t s);
 void launch_krylov_post(KrylovScalars* ks, const double* partials, int nblocks, cudaStream_t s);
+// Last node of the device loop's body: counts the body run and sets the
+// while-condition to (state == running and runs < max_it).
+void launch_krylov_cond(KrylovScalars* ks, cudaGraphConditionalHandle h, cudaStream_t s);
 
 }  // namespace cfdg

@@ -222,6 +222,7 @@ BsrSystem::BsrSystem(int device, int32_t n, int32_t bs, const int32_t* row_ptr, 
 }
 
 BsrSystem::~BsrSystem() {
+    release_device_loop();
     if (ks_host_) cudaFreeHost(ks_host_);
 }
 
@@ -339,18 +340,25 @@ void BsrSystem::build_ordering(int ordering) {
     };
     contiguous(fwd_off_, fr, fwd_first_);
     contiguous(bwd_off_, br, bwd_first_);
+    // colour-ordered matrix: colour g is rows [fwd_off_[g], fwd_off_[g+1]),
+    // so an earlier colour is a smaller row index and the first symmetric
+    // sweep can split each row at its diagonal (k_sgs_rows MODE 2 / 3)
+    split_ = ordering == CFDG_SGS_COLOR;
+    for (std::size_t g = 0; split_ && g < fwd_first_.size(); ++g) split_ = fwd_first_[g] == fwd_off_[g];
     // Unique-touch bytes of one pass over a group: row list, row pointers,
-    // diagonal index, off-diagonal blocks + columns, LU + pivots, r, z write,
-    // and each distinct neighbour z block once.
+    // diagonal index, off-diagonal blocks + columns, LU + pivots, r (or the
+    // own z read of MODE 3), z write, and each distinct neighbour z block
+    // once.  out[0]: full row, out[1]: no neighbours, out[2]: the split half
+    // (columns below the diagonal forward, above it backward).
     const double sa = (precision_ == CFDG_PREC_MIXED) ? 4.0 : 8.0;
     const double b2 = double(bs_) * bs_;
-    auto pass_bytes = [&](const std::vector<int32_t>& off, const std::vector<int32_t>& rows, std::vector<double>* out) {
+    auto pass_bytes = [&](const std::vector<int32_t>& off, const std::vector<int32_t>& rows, bool lower,
+                          std::vector<double>* out) {
         const int ng = static_cast<int>(off.size()) - 1;
-        out[0].assign(ng, 0.0);
-        out[1].assign(ng, 0.0);
-        std::vector<int32_t> seen(n, -1);
+        for (int m = 0; m < 3; ++m) out[m].assign(ng, 0.0);
+        std::vector<int32_t> seen(n, -1), seen_half(n, -1);
         for (int g = 0; g < ng; ++g) {
-            double offd = 0.0, nbr = 0.0;
+            double offd = 0.0, nbr = 0.0, offd_h = 0.0, nbr_h = 0.0;
             const double R = off[g + 1] - off[g];
             for (int32_t q = off[g]; q < off[g + 1]; ++q) {
                 const int32_t i = rows[q];
@@ -361,15 +369,23 @@ void BsrSystem::build_ordering(int ordering) {
                         seen[j] = g;
                         nbr += 1.0;
                     }
+                    if (lower ? j < i : j > i) {
+                        offd_h += 1.0;
+                        if (seen_half[j] != g) {
+                            seen_half[j] = g;
+                            nbr_h += 1.0;
+                        }
+                    }
                 }
             }
             const double own = R * (4.0 + b2 * sa + bs_ + 2.0 * 8.0 * bs_);  // list, LU, piv, r, z
             out[1][g] = own;
             out[0][g] = own + R * (8.0 + 4.0) + offd * (b2 * sa + 4.0) + nbr * 8.0 * bs_;
+            out[2][g] = own + R * (8.0 + 4.0) + offd_h * (b2 * sa + 4.0) + nbr_h * 8.0 * bs_;
         }
     };
-    pass_bytes(fwd_off_, fr, fwd_bytes_);
-    pass_bytes(bwd_off_, br, bwd_bytes_);
+    pass_bytes(fwd_off_, fr, true, fwd_bytes_);
+    pass_bytes(bwd_off_, br, false, bwd_bytes_);
     upload_or_throw(fwd_rows_, fr, stream_, "sgs rows");
     upload_or_throw(bwd_rows_, br, stream_, "sgs rows");
     ordering_ = ordering;
@@ -412,17 +428,19 @@ void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, doubl
     const bool color = ordering_ == CFDG_SGS_COLOR;
     // Neighbours ahead of the cursor must read zero on the first forward
     // sweep; with two colours every neighbour of the second colour is of the
-    // first colour, so no clearing is needed.
-    if (!color || nf > 2) {
+    // first colour, and the split sweep never reads them, so no clearing is
+    // needed then.
+    if (!color || (nf > 2 && !split_)) {
         ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 0, 8.0 * n_ * bs_);
         cuda_check(cudaMemsetAsync(z, 0, sizeof(double) * static_cast<std::size_t>(n_) * bs_, stream_), "memset");
     }
     for (int sw = 0; sw < sweeps_; ++sw) {
+        const bool split = split_ && sw == 0;
         for (int g = 0; g < nf; ++g) {
             int mode = 0;
             if (color) {
                 if (sw > 0 && g == 0) continue;  // equal to the last backward colour pass
-                if (sw == 0 && g == 0) mode = 1; // all neighbours still zero
+                if (sw == 0) mode = (g == 0) ? 1 : (split ? 2 : 0);  // colour 0: all neighbours still zero
             }
             ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, fwd_bytes_[mode][g]);
             const bool cg = fwd_first_[g] >= 0;
@@ -431,10 +449,10 @@ void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, doubl
         }
         for (int g = 0; g < nbk; ++g) {
             if (color && g == 0) continue;  // first backward colour == last forward colour
-            ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, bwd_bytes_[0][g]);
+            ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, bwd_bytes_[split ? 2 : 0][g]);
             const bool cg = bwd_first_[g] >= 0;
             launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, cg ? nullptr : bwd_rows_.p + bwd_off_[g], cg ? bwd_first_[g] : 0,
-                                   bwd_off_[g + 1] - bwd_off_[g], r, z, 0, active, stream_);
+                                   bwd_off_[g + 1] - bwd_off_[g], r, z, split ? 3 : 0, active, stream_);
         }
     }
 }
@@ -444,6 +462,61 @@ void BsrSystem::sgs_apply(const double* r, double* z, const int* active) {
     if (precision_ == CFDG_PREC_MIXED) sgs_apply_t<float>(vals32_.p, lu32_.p, r, z, active);
     else sgs_apply_t<double>(vals64_.p, lu64_.p, r, z, active);
     cuda_check(cudaGetLastError(), "sgs launch");
+}
+
+// The device loop: a graph holding one conditional while-node whose body is
+// one captured BiCGSTAB iteration followed by k_krylov_cond.  Captured once
+// per (preconditioner, x, b, SGS ordering and sweeps) and relaunched; a
+// capture or instantiation error leaves the host loop in charge.
+template <typename F>
+bool BsrSystem::device_loop_ready(int precond, double* x, const double* b, F&& iteration) {
+    const LoopKey key{precond, x, b, ordering_, sweeps_};
+    if (loop_exec_ && key == loop_key_) return true;
+    if (loop_failed_) return false;
+    release_device_loop();
+    cudaGraph_t g = nullptr, body = nullptr;
+    const int64_t launches0 = prof_->launches;
+    bool capturing = false;
+    try {
+        cuda_check(cudaGraphCreate(&g, 0), "graph create");
+        cuda_check(cudaGraphConditionalHandleCreate(&loop_handle_, g, 1, cudaGraphCondAssignDefault), "graph handle");
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = loop_handle_;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        cuda_check(cudaGraphAddNode(&node, g, nullptr, 0, &cp), "graph conditional node");
+        body = cp.conditional.phGraph_out[0];
+        cuda_check(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+                   "graph capture");
+        capturing = true;
+        iteration();
+        launch_krylov_cond(ks_.p, loop_handle_, stream_);
+        ++prof_->launches;
+        capturing = false;
+        cuda_check(cudaStreamEndCapture(stream_, &body), "graph capture end");
+        cuda_check(cudaGraphInstantiate(&loop_exec_, g, 0), "graph instantiate");
+    } catch (const Failure&) {
+        if (capturing) {
+            cudaGraph_t dead = nullptr;
+            cudaStreamEndCapture(stream_, &dead);
+        }
+        cudaGetLastError();
+        loop_exec_ = nullptr;
+        loop_failed_ = true;
+    }
+    loop_body_launches_ = prof_->launches - launches0;
+    prof_->launches = launches0;
+    if (g) cudaGraphDestroy(g);
+    if (!loop_exec_) return false;
+    loop_key_ = key;
+    return true;
+}
+
+void BsrSystem::release_device_loop() {
+    if (loop_exec_) cudaGraphExecDestroy(loop_exec_);
+    loop_exec_ = nullptr;
 }
 
 cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_tol, int max_it, double* x,
@@ -482,9 +555,9 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
     }
     const int nblk = spmv_blocks(n_, bs_);
     const int nvec = dot_blocks(N);
-    int it = 0;
-    bool done = false;
-    while (!done && it < max_it) {
+    // One BiCGSTAB iteration (bicgstab.cpp:84-176); every kernel is gated by
+    // the device-side state, so a launch after convergence does nothing.
+    auto iteration = [&]() {
         {
             ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_);
             launch_krylov_begin(ks_.p, stream_);
@@ -523,11 +596,24 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
             launch_krylov_update(N, ks_.p, x, phat, shat, s_.p, t_.p, r_.p, p_.p, v_.p, partials_.p, stream_);
             launch_krylov_post(ks_.p, partials_.p, nvec, stream_);
         }
-        ++it;
-        if (it % check_every == 0 || it == max_it) {
-            cuda_check(cudaMemcpyAsync(ks_host_, ks_.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, stream_), "D2H");
-            cuda_check(cudaStreamSynchronize(stream_), "krylov sync");
-            if (ks_host_->state != KS_RUNNING) done = true;
+    };
+    if (device_loop && !prof_->on() && max_it > 0 && device_loop_ready(precond, x, b, iteration)) {
+        cuda_check(cudaGraphLaunch(loop_exec_, stream_), "krylov graph launch");
+        cuda_check(cudaMemcpyAsync(ks_host_, ks_.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, stream_), "D2H");
+        cuda_check(cudaStreamSynchronize(stream_), "krylov sync");
+        prof_->launches += loop_body_launches_ * ks_host_->body_runs;
+    } else {
+        int it = 0;
+        bool done = false;
+        while (!done && it < max_it) {
+            iteration();
+            ++it;
+            if (it % check_every == 0 || it == max_it) {
+                cuda_check(cudaMemcpyAsync(ks_host_, ks_.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, stream_),
+                           "D2H");
+                cuda_check(cudaStreamSynchronize(stream_), "krylov sync");
+                if (ks_host_->state != KS_RUNNING) done = true;
+            }
         }
     }
     {
@@ -568,6 +654,8 @@ Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, c
     nv_ = sa_ ? 6 : 5;
     if (cfg.jacobian != CFDG_JAC_REFERENCE && cfg.jacobian != CFDG_JAC_THIN_LAYER)
         throw Failure{CFDG_ERR_INVALID, "unknown Jacobian variant"};
+    if (cfg.krylov_loop != CFDG_KRYLOV_DEVICE_LOOP && cfg.krylov_loop != CFDG_KRYLOV_HOST_LOOP)
+        throw Failure{CFDG_ERR_INVALID, "unknown Krylov loop driver"};
     muscl_ = cfg.reconstruction == CFDG_RECON_MUSCL;
     need_grad_ = muscl_ || cfg.viscous;
     if (cfg.gradient != CFDG_GRAD_LSQ_FACE && cfg.gradient != CFDG_GRAD_LSQ_NODE && need_grad_)
@@ -883,21 +971,18 @@ void Solver::setup_matrix(const HostMesh& hm, const Csr& c2c) {
         row_ptr[r + 1] = static_cast<int32_t>(cols.size());
     }
     sys_ = std::make_unique<BsrSystem>(device_, n, nv_, row_ptr.data(), cols.data(), cfg_.precision, stream_);
+    sys_->device_loop = cfg_.krylov_loop == CFDG_KRYLOV_DEVICE_LOOP;
     auto pos = [&](int32_t row, int32_t col) -> int32_t {
         const auto b = cols.begin() + row_ptr[row], e = cols.begin() + row_ptr[row + 1];
         const auto it = std::lower_bound(b, e, col);
         if (it == e || *it != col) throw Failure{CFDG_ERR_MESH, "dual graph misses a face neighbour"};
         return static_cast<int32_t>(it - cols.begin());
     };
-    std::vector<int32_t> trans(cols.size());
-    for (int32_t i = 0; i < n; ++i)
-        for (int32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) trans[k] = pos(cols[k], i);
     std::vector<int32_t> fpos(static_cast<std::size_t>(2) * hm.n_inner);
     for (int32_t f = 0; f < hm.n_inner; ++f) {
         fpos[2 * f] = pos(R(hm.owner[f]), R(hm.neigh[f]));
         fpos[2 * f + 1] = pos(R(hm.neigh[f]), R(hm.owner[f]));
     }
-    upload_or_throw(trans_, trans, stream_, "trans");
     upload_or_throw(face_pos_, fpos, stream_, "face_pos");
     if (perm) {
         upload_or_throw(row_of_, row_of_h_, stream_, "row_of");
@@ -1169,7 +1254,6 @@ void Solver::assemble_jacobian() {
     js.row_ptr = v.row_ptr;
     js.cols = v.cols;
     js.diag = v.diag;
-    js.trans = trans_.p;
     js.face_pos = face_pos_.p;
     js.full_viscous = cfg_.jacobian == CFDG_JAC_THIN_LAYER;
     js.sa_jac = sa_ ? sa_jac_.p : nullptr;

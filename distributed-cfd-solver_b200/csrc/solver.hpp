@@ -145,10 +145,14 @@ public:
     int64_t launches() const { return prof_->launches; }
     void set_profiler(Profiler* p) { prof_ = p ? p : &own_prof_; }
     Profiler* profiler() { return prof_; }
-    int check_every = 1;  // host polls the Krylov state every k iterations
+    int check_every = 1;  // host loop: polls the Krylov state every k iterations
+    bool device_loop = true;  // run the iterations as one graph launch (CFDG_KRYLOV_DEVICE_LOOP)
 
 private:
     void build_ordering(int ordering);
+    template <typename F>
+    bool device_loop_ready(int precond, double* x, const double* b, F&& iteration);
+    void release_device_loop();
     template <typename MT>
     void sgs_apply_t(const MT* vals, const MT* lu, const double* r, double* z, const int* active);
 
@@ -169,13 +173,30 @@ private:
     bool lu_ready_ = false;
     std::vector<int32_t> fwd_off_, bwd_off_;
     std::vector<int32_t> fwd_first_, bwd_first_;  // first row of a contiguous group, -1 otherwise
-    std::vector<double> fwd_bytes_[2], bwd_bytes_[2];  // algorithmic bytes of one pass, mode 0 / mode 1
+    std::vector<double> fwd_bytes_[3], bwd_bytes_[3];  // algorithmic bytes of one pass, mode 0 / 1 / split half
+    bool split_ = false;  // colour-ordered matrix: first sweep split at the diagonal
     DevArray<int32_t> fwd_rows_, bwd_rows_;
     double spmv_bytes(int n_extra_vectors, bool read_y) const;
     // Krylov workspace
     DevArray<double> r_, r0_, p_, v_, s_, t_, phat_, shat_, partials_;
     DevArray<KrylovScalars> ks_;
     KrylovScalars* ks_host_ = nullptr;
+    // device loop (graph with a conditional while-node), keyed by what the
+    // captured launches read
+    struct LoopKey {
+        int precond = -1;
+        const double* x = nullptr;
+        const double* b = nullptr;
+        int ordering = -1, sweeps = 0;
+        bool operator==(const LoopKey& o) const {
+            return precond == o.precond && x == o.x && b == o.b && ordering == o.ordering && sweeps == o.sweeps;
+        }
+    };
+    LoopKey loop_key_;
+    cudaGraphExec_t loop_exec_ = nullptr;
+    cudaGraphConditionalHandle loop_handle_{};
+    int64_t loop_body_launches_ = 0;
+    bool loop_failed_ = false;
     Profiler own_prof_;
     Profiler* prof_ = &own_prof_;
 };
@@ -254,7 +275,7 @@ private:
     double* gnu_ = nullptr;
     // linear system
     std::unique_ptr<BsrSystem> sys_;
-    DevArray<int32_t> trans_, face_pos_, row_of_, cell_of_;
+    DevArray<int32_t> face_pos_, row_of_, cell_of_;
     std::vector<int32_t> row_of_h_, cell_of_h_;  // colour-ordered system: cell -> row, row -> cell
     DevArray<double> b_, du_, norm_partials_, l2_;
     double* l2_host_ = nullptr;

@@ -156,6 +156,9 @@ typedef struct cfdg_bc_desc {
  * the owner derivative; the residual is the same. */
 enum { CFDG_JAC_REFERENCE = 0, CFDG_JAC_THIN_LAYER = 1 };
 
+/* BiCGSTAB iteration driver (cfdg_config.krylov_loop). */
+enum { CFDG_KRYLOV_DEVICE_LOOP = 0, CFDG_KRYLOV_HOST_LOOP = 1 };
+
 /* Solver configuration: SolverConfig + linalg::SolverParams
  * (include/cfd/solver/compressible/config.hpp:94-136, linalg/config.hpp:14-26)
  * plus the CFL ramp, precision, SGS ordering, SA and learned-guess options. */
@@ -182,7 +185,12 @@ typedef struct cfdg_config {
     /* run_steady freezes the MUSCL limiter values from this iteration on
      * (0 = never); cfdg_solver_freeze_limiter does it from the host loop */
     int32_t limiter_freeze;
-    int32_t reserved_;
+    /* CFDG_KRYLOV_DEVICE_LOOP: the BiCGSTAB iterations run as one CUDA graph
+     * whose conditional while-node repeats the iteration until the device-side
+     * state stops it (no host round trip per iteration; profiling switches to
+     * the host loop); CFDG_KRYLOV_HOST_LOOP: one launch sequence per
+     * iteration with the host reading the state after each. */
+    int32_t krylov_loop;
     double gamma, gas_constant, prandtl, prandtl_turb;
     double init_rho, init_p, init_velocity[3];
     double venkat_k;

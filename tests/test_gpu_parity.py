@@ -199,3 +199,73 @@ def test_thin_layer_jacobian_matches_oracle(cb):
         s.compute_dt(7.5)
         s.assemble_jacobian()
         assert rel_err(s.get(cb.FIELD_JAC), vals_ref, 25) < 1e-9
+
+
+def _colour_ordered(row_ptr, cols, vals, bs=5):
+    """The matrix with its rows and columns permuted so that the greedy
+    colouring (natural order) lists colour 0 first, then colour 1, ..."""
+    n = len(row_ptr) - 1
+    colour = np.full(n, -1)
+    for i in range(n):
+        used = {colour[j] for j in cols[row_ptr[i]:row_ptr[i + 1]] if j != i and colour[j] >= 0}
+        c = 0
+        while c in used:
+            c += 1
+        colour[i] = c
+    order = np.argsort(colour, kind="stable")  # new row -> old row
+    new_of = np.empty(n, dtype=np.int64)
+    new_of[order] = np.arange(n)
+    blocks = vals.reshape(-1, bs, bs)
+    rp, cl, vb = np.zeros(n + 1, dtype=np.int32), [], []
+    for r, i in enumerate(order):
+        ks = np.arange(row_ptr[i], row_ptr[i + 1])
+        cnew = new_of[cols[ks]]
+        srt = np.argsort(cnew)
+        cl.extend(cnew[srt])
+        vb.append(blocks[ks[srt]])
+        rp[r + 1] = len(cl)
+    return rp, np.array(cl, dtype=np.int32), np.concatenate(vb).ravel(), int(colour.max()) + 1
+
+
+@pytest.mark.parametrize("name", ["ramp_muscl", "bump_tets"])
+def test_colour_sgs_split_sweep_matches_sequential_sweep(cb, refh, name):
+    """On a colour-ordered matrix the multicolour sweep is the sequential
+    sweep (rows of one colour are independent), so the split first sweep
+    (forward below the diagonal, backward correction above it) must agree
+    with the reference's natural-order SGS to round-off, for one and two
+    sweeps."""
+    row_ptr, cols, vals = _matrix_from_ref(cb, refh, name)
+    rp, cl, vb, ncol = _colour_ordered(row_ptr, cols, vals)
+    n = len(rp) - 1
+    x = np.random.default_rng(11).standard_normal(n * 5)
+    A = cb.Bsr(rp, cl, 5)
+    A.set_values(vb)
+    for sweeps in (1, 2):
+        A.sgs_setup(cb.SGS_COLOR, sweeps)
+        z = A.sgs_apply(x)
+        z_ref = refh.sgs_apply(rp, cl, vb, 5, x, sweeps=sweeps)
+        assert rel_err(z, z_ref) < 1e-12, (sweeps, ncol)
+    if name == "bump_tets":
+        assert ncol > 2  # more than two colours: the split skips blocks the full sweep reads
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_device_loop_matches_host_loop(cb, mixed):
+    """The BiCGSTAB iterations run as one graph launch (conditional while
+    node) or one launch sequence per iteration with a host poll: the same
+    kernels in the same order, so the Newton iterates are bitwise equal."""
+    case = cb.cases.bump(scale=16, mixed=mixed)
+    mesh = cb.HostMesh(case.spec)
+    outs = []
+    for loop in (cb.KRYLOV_DEVICE_LOOP, cb.KRYLOV_HOST_LOOP):
+        case.cfg.krylov_loop = loop
+        its = []
+        with cb.Solver(mesh, case.cfg, case.bcs) as s:
+            s.init_fields()
+            for k in range(12):
+                st = s.newton_step(cb.cases.cfl_at(case.cfg, k + 1))
+                its.append(st.krylov_iterations)
+            outs.append((its, s.get(cb.FIELD_U)))
+    assert outs[0][0] == outs[1][0]
+    assert max(outs[0][0]) > 1
+    assert np.array_equal(outs[0][1], outs[1][1])
