@@ -86,8 +86,10 @@ struct BsrView {
     const int32_t* cols;
     const int32_t* diag;
 };
+// inverse: store D^-1 instead of the pivoted LU factors (multicolour sweep)
 template <typename MT>
-void launch_lu_setup(const BsrView& A, const MT* vals, MT* lu, int8_t* piv, int* err_flag, cudaStream_t s);
+void launch_lu_setup(const BsrView& A, const MT* vals, MT* lu, int8_t* piv, int* err_flag, bool inverse,
+                     cudaStream_t s);
 int spmv_blocks(int32_t n, int32_t bs);
 int dot_blocks(int64_t len);
 

@@ -87,7 +87,10 @@ __global__ void __launch_bounds__(kVecThreads) k_spmv(BsrView A, const MT* __res
 // coalesced.
 constexpr int kLuThreads = 128;
 
-template <typename MT, int BS>
+// INV: the factors are used once more to form the explicit inverse D^-1
+// (A x = e_c column by column), which is stored instead of the factors; the
+// multicolour sweep then applies D^-1 as a block-row product.
+template <typename MT, int BS, bool INV>
 __global__ void __launch_bounds__(kLuThreads) k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu,
                                                    int8_t* __restrict__ piv, int* __restrict__ err) {
     constexpr int B2 = BS * BS;
@@ -148,8 +151,39 @@ __global__ void __launch_bounds__(kLuThreads) k_lu(BsrView A, const MT* __restri
     }
     __syncthreads();  // every thread has read its block
     if (act) {
+        if constexpr (INV) {
 #pragma unroll
-        for (int e = 0; e < BS * BS; ++e) sm[threadIdx.x * B2 + e] = static_cast<MT>(a[e]);
+            for (int c = 0; c < BS; ++c) {
+                double x[BS];
+#pragma unroll
+                for (int j = 0; j < BS; ++j) x[j] = (j == c) ? 1.0 : 0.0;
+#pragma unroll
+                for (int k = 0; k < BS; ++k) {
+#pragma unroll
+                    for (int j = k + 1; j < BS; ++j)
+                        if (j == pv[k]) {
+                            const double t = x[k];
+                            x[k] = x[j];
+                            x[j] = t;
+                        }
+                }
+#pragma unroll
+                for (int r = 1; r < BS; ++r)
+#pragma unroll
+                    for (int j = 0; j < r; ++j) x[r] -= a[r * BS + j] * x[j];
+#pragma unroll
+                for (int r = BS - 1; r >= 0; --r) {
+#pragma unroll
+                    for (int j = r + 1; j < BS; ++j) x[r] -= a[r * BS + j] * x[j];
+                    x[r] = x[r] / a[r * BS + r];
+                }
+#pragma unroll
+                for (int r = 0; r < BS; ++r) sm[threadIdx.x * B2 + r * BS + c] = static_cast<MT>(x[r]);
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < BS * BS; ++e) sm[threadIdx.x * B2 + e] = static_cast<MT>(a[e]);
+        }
 #pragma unroll
         for (int k = 0; k < BS; ++k) piv[int64_t(i) * BS + k] = pv[k];
         // +(i+1): zero pivot (singular block); -(i+1): non-finite entries
@@ -206,6 +240,8 @@ __device__ __forceinline__ void lu_solve(const MT* __restrict__ lu, const int8_t
 // ascending order, as the sequential sweep), the group exchanges s by warp
 // shuffles, and each lane solves the pivoted LU system and keeps its entry.
 // MODE 1 skips the neighbour sum (all neighbour z are still zero).
+// INV: `lu` holds the explicit inverse D^-1 (multicolour ordering), applied
+// as a block-row product: five loads per lane instead of the whole factor.
 // MODE 2 and 3 are the two halves of the first symmetric sweep of a
 // colour-ordered matrix (every colour a contiguous row range, colours
 // ascending, so "column < row" means "earlier colour"):
@@ -214,7 +250,7 @@ __device__ __forceinline__ void lu_solve(const MT* __restrict__ lu, const int8_t
 // which equals the full-row backward update D_i^-1 (r_i - sum_lower A y -
 // sum_upper A z) because (D + L) y = r, and reads neither r nor the lower
 // blocks.
-template <typename MT, int BS, int MODE>
+template <typename MT, int BS, int MODE, bool INV>
 __global__ void __launch_bounds__(256) k_sgs_rows(BsrView A, const MT* __restrict__ vals, const MT* __restrict__ lu,
                                                   const int8_t* __restrict__ piv, const int32_t* __restrict__ rows,
                                                   int32_t row0, int32_t n_rows, const double* __restrict__ r,
@@ -251,11 +287,19 @@ __global__ void __launch_bounds__(256) k_sgs_rows(BsrView A, const MT* __restric
 #pragma unroll
     for (int j = 0; j < BS; ++j) b[j] = __shfl_sync(0xffffffffu, s, base + j);
     if (act) {
-        lu_solve<MT, BS>(lu + int64_t(i) * (BS * BS), piv + int64_t(i) * BS, b);
-        double out = b[0];
+        double out;
+        if constexpr (INV) {  // row ii of D^-1 times s
+            const MT* di = lu + int64_t(i) * (BS * BS) + ii * BS;
+            out = 0.0;
 #pragma unroll
-        for (int j = 1; j < BS; ++j)
-            if (j == ii) out = b[j];
+            for (int j = 0; j < BS; ++j) out += ld(di + j) * b[j];
+        } else {
+            lu_solve<MT, BS>(lu + int64_t(i) * (BS * BS), piv + int64_t(i) * BS, b);
+            out = b[0];
+#pragma unroll
+            for (int j = 1; j < BS; ++j)
+                if (j == ii) out = b[j];
+        }
         // MODE 3: b solved D x = -sum_upper A z, so z_i = y_i + x
         if (MODE == 3) out = z[int64_t(i) * BS + ii] + out;
         z[int64_t(i) * BS + ii] = out;
@@ -504,31 +548,39 @@ void launch_spmv_ex(const BsrView& A, const MT* vals, const double* x, double* y
 }
 
 template <typename MT>
-void launch_lu_setup(const BsrView& A, const MT* vals, MT* lu, int8_t* piv, int* err_flag, cudaStream_t s) {
+void launch_lu_setup(const BsrView& A, const MT* vals, MT* lu, int8_t* piv, int* err_flag, bool inverse,
+                     cudaStream_t s) {
     const unsigned gr = grid_for(A.n, kLuThreads);
+#define CFDG_LU(BS)                                                                          \
+    if (inverse) k_lu<MT, BS, true><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); \
+    else k_lu<MT, BS, false><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag)
     switch (A.bs) {
-        case 1: k_lu<MT, 1><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
-        case 3: k_lu<MT, 3><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
-        case 4: k_lu<MT, 4><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
-        case 5: k_lu<MT, 5><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
-        case 6: k_lu<MT, 6><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); break;
+        case 1: CFDG_LU(1); break;
+        case 3: CFDG_LU(3); break;
+        case 4: CFDG_LU(4); break;
+        case 5: CFDG_LU(5); break;
+        case 6: CFDG_LU(6); break;
         default: break;
     }
+#undef CFDG_LU
 }
 
 template <typename MT>
 void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* rows,
-                        int32_t row0, int32_t n_rows, const double* r, double* z, int mode, const int* active,
-                        cudaStream_t s) {
+                        int32_t row0, int32_t n_rows, const double* r, double* z, int mode, bool inverse,
+                        const int* active, cudaStream_t s) {
     if (n_rows <= 0) return;
     const int gpw = 32 / A.bs;
     const int64_t warps = (int64_t(n_rows) + gpw - 1) / gpw;
     const unsigned gr = grid_for(warps * 32, 256);
-#define CFDG_SGS(BS)                                                                                            \
-    if (mode == 0) k_sgs_rows<MT, BS, 0><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active);   \
-    else if (mode == 1) k_sgs_rows<MT, BS, 1><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active); \
-    else if (mode == 2) k_sgs_rows<MT, BS, 2><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active); \
-    else k_sgs_rows<MT, BS, 3><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active)
+#define CFDG_SGS_M(BS, M)                                                                                      \
+    if (inverse) k_sgs_rows<MT, BS, M, true><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active); \
+    else k_sgs_rows<MT, BS, M, false><<<gr, 256, 0, s>>>(A, vals, lu, piv, rows, row0, n_rows, r, z, active)
+#define CFDG_SGS(BS)                           \
+    if (mode == 0) { CFDG_SGS_M(BS, 0); }      \
+    else if (mode == 1) { CFDG_SGS_M(BS, 1); } \
+    else if (mode == 2) { CFDG_SGS_M(BS, 2); } \
+    else { CFDG_SGS_M(BS, 3); }
     switch (A.bs) {
         case 1: CFDG_SGS(1); break;
         case 3: CFDG_SGS(3); break;
@@ -538,6 +590,7 @@ void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const in
         default: break;
     }
 #undef CFDG_SGS
+#undef CFDG_SGS_M
 }
 
 int dot_blocks(int64_t len) { return static_cast<int>(vec_grid(len)); }
@@ -592,12 +645,14 @@ template void launch_spmv_ex<double>(const BsrView&, const double*, const double
                                      const DotSpec&, double*, const int*, cudaStream_t);
 template void launch_spmv_ex<float>(const BsrView&, const float*, const double*, double*, double, double,
                                     const DotSpec&, double*, const int*, cudaStream_t);
-template void launch_lu_setup<double>(const BsrView&, const double*, double*, int8_t*, int*, cudaStream_t);
-template void launch_lu_setup<float>(const BsrView&, const float*, float*, int8_t*, int*, cudaStream_t);
+template void launch_lu_setup<double>(const BsrView&, const double*, double*, int8_t*, int*, bool, cudaStream_t);
+template void launch_lu_setup<float>(const BsrView&, const float*, float*, int8_t*, int*, bool, cudaStream_t);
 template void launch_sgs_rows_ex<double>(const BsrView&, const double*, const double*, const int8_t*, const int32_t*,
-                                         int32_t, int32_t, const double*, double*, int, const int*, cudaStream_t);
+                                         int32_t, int32_t, const double*, double*, int, bool, const int*,
+                                         cudaStream_t);
 template void launch_sgs_rows_ex<float>(const BsrView&, const float*, const float*, const int8_t*, const int32_t*,
-                                        int32_t, int32_t, const double*, double*, int, const int*, cudaStream_t);
+                                        int32_t, int32_t, const double*, double*, int, bool, const int*,
+                                        cudaStream_t);
 
 void launch_krylov_cond(KrylovScalars* ks, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_krylov_cond<<<1, 32, 0, s>>>(ks, h);

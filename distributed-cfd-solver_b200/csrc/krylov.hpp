@@ -35,10 +35,11 @@ template <typename MT>
 void launch_spmv_ex(const BsrView& A, const MT* vals, const double* x, double* y, double alpha, double beta,
                     const DotSpec& ds, double* partials, const int* active, cudaStream_t s);
 // rows: the pass's row list, or null for the contiguous rows row0 ..
+// inverse: `lu` holds D^-1 (launch_lu_setup with inverse)
 template <typename MT>
 void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* rows,
-                        int32_t row0, int32_t n_rows, const double* r, double* z, int mode, const int* active,
-                        cudaStream_t s);
+                        int32_t row0, int32_t n_rows, const double* r, double* z, int mode, bool inverse,
+                        const int* active, cudaStream_t s);
 void launch_krylov_init(int64_t len, const double* b, const double* v, double* r, double* r0, double* p,
                         double* partials, KrylovScalars* ks, cudaStream_t s);
 // After launch_krylov_init: a rejected initial guess (||b - A x0|| >=

@@ -378,7 +378,8 @@ void BsrSystem::build_ordering(int ordering) {
                     }
                 }
             }
-            const double own = R * (4.0 + b2 * sa + bs_ + 2.0 * 8.0 * bs_);  // list, LU, piv, r, z
+            // list, LU factors + pivots (level) or D^-1 (colour), r, z
+            const double own = R * (4.0 + b2 * sa + (ordering == CFDG_SGS_COLOR ? 0.0 : bs_) + 2.0 * 8.0 * bs_);
             out[1][g] = own;
             out[0][g] = own + R * (8.0 + 4.0) + offd * (b2 * sa + 4.0) + nbr * 8.0 * bs_;
             out[2][g] = own + R * (8.0 + 4.0) + offd_h * (b2 * sa + 4.0) + nbr_h * 8.0 * bs_;
@@ -402,11 +403,11 @@ void BsrSystem::sgs_setup(int ordering, int sweeps) {
     if (precision_ == CFDG_PREC_MIXED) {
         if (!lu32_.p && n_ > 0) alloc_or_throw(lu32_, nb2, "lu");
         ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1, double(n_) * (bs_ * bs_ * 8.0 + bs_ + 4.0));
-        launch_lu_setup<float>(view(), vals32_.p, lu32_.p, piv_.p, err_.p, stream_);
+        launch_lu_setup<float>(view(), vals32_.p, lu32_.p, piv_.p, err_.p, ordering_ == CFDG_SGS_COLOR, stream_);
     } else {
         if (!lu64_.p && n_ > 0) alloc_or_throw(lu64_, nb2, "lu");
         ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1, double(n_) * (bs_ * bs_ * 16.0 + bs_ + 4.0));
-        launch_lu_setup<double>(view(), vals64_.p, lu64_.p, piv_.p, err_.p, stream_);
+        launch_lu_setup<double>(view(), vals64_.p, lu64_.p, piv_.p, err_.p, ordering_ == CFDG_SGS_COLOR, stream_);
     }
     cuda_check(cudaGetLastError(), "lu launch");
     int err = 0;
@@ -445,14 +446,14 @@ void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, doubl
             ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, fwd_bytes_[mode][g]);
             const bool cg = fwd_first_[g] >= 0;
             launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, cg ? nullptr : fwd_rows_.p + fwd_off_[g], cg ? fwd_first_[g] : 0,
-                                   fwd_off_[g + 1] - fwd_off_[g], r, z, mode, active, stream_);
+                                   fwd_off_[g + 1] - fwd_off_[g], r, z, mode, color, active, stream_);
         }
         for (int g = 0; g < nbk; ++g) {
             if (color && g == 0) continue;  // first backward colour == last forward colour
             ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, bwd_bytes_[split ? 2 : 0][g]);
             const bool cg = bwd_first_[g] >= 0;
             launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, cg ? nullptr : bwd_rows_.p + bwd_off_[g], cg ? bwd_first_[g] : 0,
-                                   bwd_off_[g + 1] - bwd_off_[g], r, z, split ? 3 : 0, active, stream_);
+                                   bwd_off_[g + 1] - bwd_off_[g], r, z, split ? 3 : 0, color, active, stream_);
         }
     }
 }

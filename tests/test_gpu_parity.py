@@ -233,7 +233,9 @@ def test_colour_sgs_split_sweep_matches_sequential_sweep(cb, refh, name):
     sweep (rows of one colour are independent), so the split first sweep
     (forward below the diagonal, backward correction above it) must agree
     with the reference's natural-order SGS to round-off, for one and two
-    sweeps."""
+    sweeps.  The multicolour sweep applies the explicit inverse of each
+    diagonal block instead of its pivoted LU factors: 1e-10 covers the
+    condition number of the blocks times the FP64 rounding."""
     row_ptr, cols, vals = _matrix_from_ref(cb, refh, name)
     rp, cl, vb, ncol = _colour_ordered(row_ptr, cols, vals)
     n = len(rp) - 1
@@ -244,7 +246,7 @@ def test_colour_sgs_split_sweep_matches_sequential_sweep(cb, refh, name):
         A.sgs_setup(cb.SGS_COLOR, sweeps)
         z = A.sgs_apply(x)
         z_ref = refh.sgs_apply(rp, cl, vb, 5, x, sweeps=sweeps)
-        assert rel_err(z, z_ref) < 1e-12, (sweeps, ncol)
+        assert rel_err(z, z_ref) < 1e-10, (sweeps, ncol)
     if name == "bump_tets":
         assert ncol > 2  # more than two colours: the split skips blocks the full sweep reads
 
