@@ -251,7 +251,7 @@ __device__ __forceinline__ void lu_solve(const MT* __restrict__ lu, const int8_t
 // sum_upper A z) because (D + L) y = r, and reads neither r nor the lower
 // blocks.
 template <typename MT, int BS, int MODE, bool INV>
-__global__ void __launch_bounds__(256) k_sgs_rows(BsrView A, const MT* __restrict__ vals, const MT* __restrict__ lu,
+__global__ void __launch_bounds__(256, (INV && BS <= 5) ? 8 : 6) k_sgs_rows(BsrView A, const MT* __restrict__ vals, const MT* __restrict__ lu,
                                                   const int8_t* __restrict__ piv, const int32_t* __restrict__ rows,
                                                   int32_t row0, int32_t n_rows, const double* __restrict__ r,
                                                   double* __restrict__ z, const int* __restrict__ active) {
