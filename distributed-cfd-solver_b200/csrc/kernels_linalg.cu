@@ -38,18 +38,21 @@ inline unsigned vec_grid(int64_t len) {
 // One thread per (block row, component): y_i[ii] = alpha * sum_k sum_jj
 // A_k[ii][jj] x_col(k)[jj] + beta * y.  Optional fused dot products of y
 // (or other vectors) for the Krylov scalars, reduced per block.
+// Rows [row_begin, n) (row_begin > 0: the rows left after the fused
+// product of the last SGS pass).
 template <typename MT, int BS, int ND>
 __global__ void __launch_bounds__(kVecThreads) k_spmv(BsrView A, const MT* __restrict__ vals,
                                                       const double* __restrict__ x, double* __restrict__ y,
                                                       double alpha, double beta, DotSpec ds,
-                                                      double* __restrict__ partials, const int* __restrict__ active) {
+                                                      double* __restrict__ partials, const int* __restrict__ active,
+                                                      int32_t row_begin) {
     if (active && *active != 0) return;
     const int64_t N = int64_t(A.n) * BS;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     double pr[ND > 0 ? ND : 1];
 #pragma unroll
     for (int k = 0; k < (ND > 0 ? ND : 1); ++k) pr[k] = 0.0;
-    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < N; t += stride) {
+    for (int64_t t = int64_t(row_begin) * BS + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < N; t += stride) {
         const int32_t row = static_cast<int32_t>(t / BS);
         const int ii = static_cast<int>(t % BS);
         double acc = 0.0;
@@ -306,6 +309,81 @@ __global__ void __launch_bounds__(256, (INV && BS <= 5) ? 8 : 6) k_sgs_rows(BsrV
     }
 }
 
+// The last backward pass of a split multicolour sweep (colour 0, rows
+// [0, n_rows), every neighbour of a later colour and already final) fused
+// with the product y = A z on those rows.  The pass computes
+// t = sum_{k > diag} A_ik z_k and z_i = y_i - D_i^-1 t (MODE 3 with D^-1);
+// all of row i's off-diagonal blocks are then in t, so
+// (A z)_i = t + A_ii z_i costs one more block instead of the row's blocks
+// again.  Dot products of the result as k_spmv; the grid strides over the
+// rows so the partials number at most kVecGridCap.
+template <typename MT, int BS, int ND>
+__global__ void __launch_bounds__(256, BS <= 5 ? 8 : 6) k_sgs_last_spmv(BsrView A, const MT* __restrict__ vals,
+                                                                       const MT* __restrict__ dinv, int32_t n_rows,
+                                                                       double* __restrict__ z, double* __restrict__ y,
+                                                                       DotSpec ds, double* __restrict__ partials,
+                                                                       const int* __restrict__ active) {
+    if (active && *active != 0) return;
+    constexpr int GPW = 32 / BS;
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / BS, ii = lane - grp * BS;
+    const int base = (grp < GPW ? grp : 0) * BS;
+    const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    double pr[ND > 0 ? ND : 1];
+#pragma unroll
+    for (int k = 0; k < (ND > 0 ? ND : 1); ++k) pr[k] = 0.0;
+    for (int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w * GPW < n_rows; w += warps) {
+        const int64_t slot = w * GPW + grp;
+        const bool act = (grp < GPW) && (slot < n_rows);
+        const int32_t i = act ? static_cast<int32_t>(slot) : 0;
+        double s = 0.0;
+        if (act) {
+            const int32_t k1 = A.row_ptr[i + 1];
+            for (int32_t k = A.diag[i] + 1; k < k1; ++k) {
+                const MT* a = vals + int64_t(k) * (BS * BS) + ii * BS;
+                const double* zb = z + int64_t(A.cols[k]) * BS;
+                double t = 0.0;
+#pragma unroll
+                for (int jj = 0; jj < BS; ++jj) t += ld(a + jj) * zb[jj];
+                s -= t;
+            }
+        }
+        double b[BS];
+#pragma unroll
+        for (int j = 0; j < BS; ++j) b[j] = __shfl_sync(0xffffffffu, s, base + j);
+        double zi = 0.0;
+        if (act) {
+            const MT* di = dinv + int64_t(i) * (BS * BS) + ii * BS;
+            double x = 0.0;
+#pragma unroll
+            for (int j = 0; j < BS; ++j) x += ld(di + j) * b[j];
+            zi = z[int64_t(i) * BS + ii] + x;
+            z[int64_t(i) * BS + ii] = zi;
+        }
+        double zr[BS];
+#pragma unroll
+        for (int j = 0; j < BS; ++j) zr[j] = __shfl_sync(0xffffffffu, zi, base + j);
+        if (act) {
+            const MT* ad = vals + int64_t(A.diag[i]) * (BS * BS) + ii * BS;
+            double d = 0.0;
+#pragma unroll
+            for (int jj = 0; jj < BS; ++jj) d += ld(ad + jj) * zr[jj];
+            const double yv = d - s;
+            const int64_t t = int64_t(i) * BS + ii;
+            y[t] = yv;
+            if constexpr (ND > 0) {
+#pragma unroll
+                for (int k = 0; k < ND; ++k) {
+                    const double a = ds.a[k] ? ds.a[k][t] : yv;
+                    const double bb = ds.b[k] ? ds.b[k][t] : yv;
+                    pr[k] += a * bb;
+                }
+            }
+        }
+    }
+    if constexpr (ND > 0) block_reduce_store<ND, 256>(pr, partials + size_t(blockIdx.x) * ND);
+}
+
 // ------------------------------------------------------ Krylov kernels
 // r = b - v, r0 = r, p = r; partial sums of |b|^2 and |r|^2.
 __global__ void __launch_bounds__(kVecThreads) k_krylov_init(int64_t len, const double* __restrict__ b,
@@ -517,12 +595,38 @@ __global__ void k_krylov_cond(KrylovScalars* ks, cudaGraphConditionalHandle h) {
 // ------------------------------------------------------------- launchers
 int spmv_blocks(int32_t n, int32_t bs) { return static_cast<int>(vec_grid(int64_t(n) * bs)); }
 
+int sgs_last_spmv_blocks(int32_t n_rows, int32_t bs) {
+    const int64_t warps = (int64_t(n_rows) + (32 / bs) - 1) / (32 / bs);
+    const int64_t g = (warps + 7) / 8;
+    return static_cast<int>(g < 1 ? 1 : (g < kVecGridCap ? g : kVecGridCap));
+}
+
+template <typename MT>
+void launch_sgs_last_spmv(const BsrView& A, const MT* vals, const MT* dinv, int32_t n_rows, double* z, double* y,
+                          const DotSpec& ds, double* partials, const int* active, cudaStream_t s) {
+    const unsigned gr = static_cast<unsigned>(sgs_last_spmv_blocks(n_rows, A.bs));
+#define CFDG_FUSED(BS)                                                                                     \
+    if (ds.n == 0) k_sgs_last_spmv<MT, BS, 0><<<gr, 256, 0, s>>>(A, vals, dinv, n_rows, z, y, ds, partials, active); \
+    else if (ds.n == 1) k_sgs_last_spmv<MT, BS, 1><<<gr, 256, 0, s>>>(A, vals, dinv, n_rows, z, y, ds, partials, active); \
+    else k_sgs_last_spmv<MT, BS, 5><<<gr, 256, 0, s>>>(A, vals, dinv, n_rows, z, y, ds, partials, active)
+    switch (A.bs) {
+        case 1: CFDG_FUSED(1); break;
+        case 3: CFDG_FUSED(3); break;
+        case 4: CFDG_FUSED(4); break;
+        case 5: CFDG_FUSED(5); break;
+        case 6: CFDG_FUSED(6); break;
+        default: break;
+    }
+#undef CFDG_FUSED
+}
+
 template <typename MT>
 void launch_spmv_ex(const BsrView& A, const MT* vals, const double* x, double* y, double alpha, double beta,
-                    const DotSpec& ds, double* partials, const int* active, cudaStream_t s) {
-    const unsigned gr = vec_grid(int64_t(A.n) * A.bs);
+                    const DotSpec& ds, double* partials, const int* active, cudaStream_t s, int32_t row_begin) {
+    const unsigned gr = vec_grid(int64_t(A.n - row_begin) * A.bs);
     const int nd = ds.n;
-#define CFDG_SPMV(BS, ND) k_spmv<MT, BS, ND><<<gr, kVecThreads, 0, s>>>(A, vals, x, y, alpha, beta, ds, partials, active)
+#define CFDG_SPMV(BS, ND) \
+    k_spmv<MT, BS, ND><<<gr, kVecThreads, 0, s>>>(A, vals, x, y, alpha, beta, ds, partials, active, row_begin)
     if (A.bs == 5) {
         if (nd == 0) CFDG_SPMV(5, 0);
         else if (nd == 1) CFDG_SPMV(5, 1);
@@ -642,9 +746,13 @@ void launch_krylov_post(KrylovScalars* ks, const double* partials, int nblocks, 
 }
 
 template void launch_spmv_ex<double>(const BsrView&, const double*, const double*, double*, double, double,
-                                     const DotSpec&, double*, const int*, cudaStream_t);
+                                     const DotSpec&, double*, const int*, cudaStream_t, int32_t);
 template void launch_spmv_ex<float>(const BsrView&, const float*, const double*, double*, double, double,
-                                    const DotSpec&, double*, const int*, cudaStream_t);
+                                    const DotSpec&, double*, const int*, cudaStream_t, int32_t);
+template void launch_sgs_last_spmv<double>(const BsrView&, const double*, const double*, int32_t, double*, double*,
+                                           const DotSpec&, double*, const int*, cudaStream_t);
+template void launch_sgs_last_spmv<float>(const BsrView&, const float*, const float*, int32_t, double*, double*,
+                                          const DotSpec&, double*, const int*, cudaStream_t);
 template void launch_lu_setup<double>(const BsrView&, const double*, double*, int8_t*, int*, bool, cudaStream_t);
 template void launch_lu_setup<float>(const BsrView&, const float*, float*, int8_t*, int*, bool, cudaStream_t);
 template void launch_sgs_rows_ex<double>(const BsrView&, const double*, const double*, const int8_t*, const int32_t*,

@@ -31,9 +31,17 @@ struct DotSpec {
     int n;
 };
 
+// y = alpha A x + beta y on rows [row_begin, n), optional fused dots
 template <typename MT>
 void launch_spmv_ex(const BsrView& A, const MT* vals, const double* x, double* y, double alpha, double beta,
-                    const DotSpec& ds, double* partials, const int* active, cudaStream_t s);
+                    const DotSpec& ds, double* partials, const int* active, cudaStream_t s, int32_t row_begin = 0);
+// Last backward pass of the split multicolour sweep (colour 0 = rows
+// [0, n_rows), `dinv` the inverse diagonal blocks) fused with y = A z and the
+// dots on those rows; partials: sgs_last_spmv_blocks(n_rows, bs) * ds.n.
+template <typename MT>
+void launch_sgs_last_spmv(const BsrView& A, const MT* vals, const MT* dinv, int32_t n_rows, double* z, double* y,
+                          const DotSpec& ds, double* partials, const int* active, cudaStream_t s);
+int sgs_last_spmv_blocks(int32_t n_rows, int32_t bs);
 // rows: the pass's row list, or null for the contiguous rows row0 ..
 // inverse: `lu` holds D^-1 (launch_lu_setup with inverse)
 template <typename MT>

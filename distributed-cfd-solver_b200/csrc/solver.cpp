@@ -215,7 +215,11 @@ BsrSystem::BsrSystem(int device, int32_t n, int32_t bs, const int32_t* row_ptr, 
     else alloc_or_throw(vals64_, nv, "values");
     const std::size_t N = static_cast<std::size_t>(n) * bs;
     for (DevArray<double>* a : {&r_, &r0_, &p_, &v_, &s_, &t_, &phat_, &shat_}) alloc_or_throw(*a, N > 0 ? N : 1, "krylov");
-    alloc_or_throw(partials_, static_cast<std::size_t>(std::max(dot_blocks(N), spmv_blocks(n, bs))) * 5 + 8, "partials");
+    // the fused colour-0 product and the SpMV of the other rows write their
+    // partials one after the other
+    alloc_or_throw(partials_,
+                   static_cast<std::size_t>(sgs_last_spmv_blocks(n, bs) + std::max(dot_blocks(N), spmv_blocks(n, bs))) * 5 + 8,
+                   "partials");
     alloc_or_throw(ks_, 1, "krylov scalars");
     alloc_or_throw(err_, 1, "error flag");
     cuda_check(cudaMallocHost(reinterpret_cast<void**>(&ks_host_), sizeof(KrylovScalars)), "cudaMallocHost");
@@ -345,6 +349,14 @@ void BsrSystem::build_ordering(int ordering) {
     // sweep can split each row at its diagonal (k_sgs_rows MODE 2 / 3)
     split_ = ordering == CFDG_SGS_COLOR;
     for (std::size_t g = 0; split_ && g < fwd_first_.size(); ++g) split_ = fwd_first_[g] == fwd_off_[g];
+    rest_nnzb_ = rest_cols_ = 0.0;
+    if (split_ && fwd_off_.size() > 2) {
+        std::vector<char> used(n, 0);
+        for (int32_t i = fwd_off_[1]; i < n; ++i)
+            for (int32_t k = row_ptr_h_[i]; k < row_ptr_h_[i + 1]; ++k) used[cols_h_[k]] = 1;
+        for (int32_t j = 0; j < n; ++j) rest_cols_ += used[j];
+        rest_nnzb_ = double(nnzb_ - row_ptr_h_[fwd_off_[1]]);
+    }
     // Unique-touch bytes of one pass over a group: row list, row pointers,
     // diagonal index, off-diagonal blocks + columns, LU + pivots, r (or the
     // own z read of MODE 3), z write, and each distinct neighbour z block
@@ -423,7 +435,8 @@ void BsrSystem::sgs_setup(int ordering, int sweeps) {
 }
 
 template <typename MT>
-void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, double* z, const int* active) {
+void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, double* z, const int* active,
+                            bool skip_last) {
     const BsrView A = view();
     const int nf = groups_fwd(), nbk = groups_bwd();
     const bool color = ordering_ == CFDG_SGS_COLOR;
@@ -450,12 +463,52 @@ void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, doubl
         }
         for (int g = 0; g < nbk; ++g) {
             if (color && g == 0) continue;  // first backward colour == last forward colour
+            if (skip_last && g == nbk - 1) continue;  // fused with the product (sgs_apply_spmv)
             ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, bwd_bytes_[split ? 2 : 0][g]);
             const bool cg = bwd_first_[g] >= 0;
             launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, cg ? nullptr : bwd_rows_.p + bwd_off_[g], cg ? bwd_first_[g] : 0,
                                    bwd_off_[g + 1] - bwd_off_[g], r, z, split ? 3 : 0, color, active, stream_);
         }
     }
+}
+
+int BsrSystem::sgs_apply_spmv(const double* r, double* z, double* y, const DotSpec& ds, double* partials,
+                              const int* active) {
+    if (!lu_ready_) throw Failure{CFDG_ERR_INVALID, "SgsPreconditioner: setup() was not called"};
+    const BsrView A = view();
+    const bool mixed = precision_ == CFDG_PREC_MIXED;
+    const double sa = mixed ? 4.0 : 8.0;
+    const double b2 = double(bs_) * bs_;
+    const int nx = ds.n == 1 ? 1 : 2;  // vectors the dots read besides y (r0; r0 and s)
+    if (!fuse_last_spmv()) {
+        sgs_apply(r, z, active);
+        ProfScope ps(prof_, CFDG_KCAT_SPMV, stream_, 1, spmv_bytes(nx, false));
+        if (mixed) launch_spmv_ex<float>(A, vals32_.p, z, y, 1.0, 0.0, ds, partials, active, stream_);
+        else launch_spmv_ex<double>(A, vals64_.p, z, y, 1.0, 0.0, ds, partials, active, stream_);
+        cuda_check(cudaGetLastError(), "spmv launch");
+        return spmv_blocks(n_, bs_);
+    }
+    if (mixed) sgs_apply_t<float>(vals32_.p, lu32_.p, r, z, active, true);
+    else sgs_apply_t<double>(vals64_.p, lu64_.p, r, z, active, true);
+    const int32_t n0 = fwd_off_[1];  // colour 0: rows [0, n0)
+    const int g0 = sgs_last_spmv_blocks(n0, bs_);
+    {
+        const double N0 = double(n0) * bs_;
+        ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1,
+                     bwd_bytes_[2][groups_bwd() - 1] + double(n0) * b2 * sa + N0 * 8.0 * (1.0 + nx));
+        if (mixed) launch_sgs_last_spmv<float>(A, vals32_.p, lu32_.p, n0, z, y, ds, partials, active, stream_);
+        else launch_sgs_last_spmv<double>(A, vals64_.p, lu64_.p, n0, z, y, ds, partials, active, stream_);
+    }
+    double* rest = partials + static_cast<std::size_t>(g0) * ds.n;
+    {
+        const double Nr = double(n_ - n0) * bs_;
+        ProfScope ps(prof_, CFDG_KCAT_SPMV, stream_, 1,
+                     rest_nnzb_ * (b2 * sa + 4.0) + (n_ - n0 + 1.0) * 4.0 + rest_cols_ * bs_ * 8.0 + Nr * 8.0 * (1.0 + nx));
+        if (mixed) launch_spmv_ex<float>(A, vals32_.p, z, y, 1.0, 0.0, ds, rest, active, stream_, n0);
+        else launch_spmv_ex<double>(A, vals64_.p, z, y, 1.0, 0.0, ds, rest, active, stream_, n0);
+    }
+    cuda_check(cudaGetLastError(), "sgs+spmv launch");
+    return g0 + spmv_blocks(n_ - n0, bs_);
 }
 
 void BsrSystem::sgs_apply(const double* r, double* z, const int* active) {
@@ -563,25 +616,22 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
             ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_);
             launch_krylov_begin(ks_.p, stream_);
         }
-        double* phat = p_.p;
-        if (precond == CFDG_PC_SGS) {
-            sgs_apply(p_.p, phat_.p, active);
-            phat = phat_.p;
-        }
         DotSpec d1{};
         d1.n = 1;
         d1.a[0] = r0_.p;
         d1.b[0] = nullptr;
-        spmv_dots(phat, v_.p, d1);
+        double* phat = p_.p;
+        int nb1 = nblk;
+        if (precond == CFDG_PC_SGS) {
+            nb1 = sgs_apply_spmv(p_.p, phat_.p, v_.p, d1, partials_.p, active);
+            phat = phat_.p;
+        } else {
+            spmv_dots(phat, v_.p, d1);
+        }
         {
             ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 2, 3.0 * 8.0 * N);
-            launch_krylov_gamma(ks_.p, partials_.p, nblk, stream_);
+            launch_krylov_gamma(ks_.p, partials_.p, nb1, stream_);
             launch_krylov_s(N, ks_.p, r_.p, v_.p, s_.p, stream_);
-        }
-        double* shat = s_.p;
-        if (precond == CFDG_PC_SGS) {
-            sgs_apply(s_.p, shat_.p, active);
-            shat = shat_.p;
         }
         DotSpec d5{};
         d5.n = 5;
@@ -590,10 +640,17 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
         d5.a[2] = r0_.p;   d5.b[2] = nullptr;   // r0.t
         d5.a[3] = r0_.p;   d5.b[3] = s_.p;      // r0.s
         d5.a[4] = s_.p;    d5.b[4] = s_.p;      // s.s
-        spmv_dots(shat, t_.p, d5);
+        double* shat = s_.p;
+        int nb5 = nblk;
+        if (precond == CFDG_PC_SGS) {
+            nb5 = sgs_apply_spmv(s_.p, shat_.p, t_.p, d5, partials_.p, active);
+            shat = shat_.p;
+        } else {
+            spmv_dots(shat, t_.p, d5);
+        }
         {
             ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 3, 10.0 * 8.0 * N);
-            launch_krylov_omega(ks_.p, partials_.p, nblk, stream_);
+            launch_krylov_omega(ks_.p, partials_.p, nb5, stream_);
             launch_krylov_update(N, ks_.p, x, phat, shat, s_.p, t_.p, r_.p, p_.p, v_.p, partials_.p, stream_);
             launch_krylov_post(ks_.p, partials_.p, nvec, stream_);
         }

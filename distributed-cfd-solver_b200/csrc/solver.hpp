@@ -133,6 +133,10 @@ public:
     void sgs_setup(int ordering, int sweeps);
     // z = M^-1 r (device vectors).
     void sgs_apply(const double* r, double* z, const int* active);
+    // z = M^-1 r, then y = A z with the dots `ds` (partials at `partials`);
+    // with the split multicolour sweep the product on colour 0 is fused into
+    // its last pass.  Returns the number of partial rows written.
+    int sgs_apply_spmv(const double* r, double* z, double* y, const DotSpec& ds, double* partials, const int* active);
     // BiCGSTAB on device vectors; x holds the initial guess.
     // guess: x holds an initial guess that is replaced by x = 0 when
     // ||b - A x|| >= ||b||; last_guess() tells 1 accepted, 2 rejected.
@@ -154,7 +158,9 @@ private:
     bool device_loop_ready(int precond, double* x, const double* b, F&& iteration);
     void release_device_loop();
     template <typename MT>
-    void sgs_apply_t(const MT* vals, const MT* lu, const double* r, double* z, const int* active);
+    void sgs_apply_t(const MT* vals, const MT* lu, const double* r, double* z, const int* active,
+                     bool skip_last = false);
+    bool fuse_last_spmv() const { return split_ && sweeps_ == 1 && groups_bwd() >= 2; }
 
     int device_;
     cudaStream_t stream_;
@@ -177,6 +183,9 @@ private:
     bool split_ = false;  // colour-ordered matrix: first sweep split at the diagonal
     DevArray<int32_t> fwd_rows_, bwd_rows_;
     double spmv_bytes(int n_extra_vectors, bool read_y) const;
+    // rows [fwd_off_[1], n) of a colour-ordered matrix: block count and
+    // distinct columns (the SpMV left after the fused colour-0 product)
+    double rest_nnzb_ = 0.0, rest_cols_ = 0.0;
     // Krylov workspace
     DevArray<double> r_, r0_, p_, v_, s_, t_, phat_, shat_, partials_;
     DevArray<KrylovScalars> ks_;

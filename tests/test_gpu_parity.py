@@ -249,6 +249,15 @@ def test_colour_sgs_split_sweep_matches_sequential_sweep(cb, refh, name):
         assert rel_err(z, z_ref) < 1e-10, (sweeps, ncol)
     if name == "bump_tets":
         assert ncol > 2  # more than two colours: the split skips blocks the full sweep reads
+    # BiCGSTAB with the split sweep, whose colour-0 pass carries the product
+    # A z of those rows: the same solution as the reference's solver
+    A.sgs_setup(cb.SGS_COLOR, 1)
+    b = np.random.default_rng(12).standard_normal(n * 5)
+    sol, info = A.bicgstab(b, precond=cb.PC_SGS, rel_tol=1e-10, max_it=400)
+    sol_ref, info_ref = refh.bicgstab(rp, cl, vb, 5, b, precond=1, rel_tol=1e-10, max_it=400)
+    assert info.status == cb.KRYLOV_CONVERGED and info_ref["status"] == 0
+    assert rel_err(sol, sol_ref) < 1e-7
+    assert rel_err(A.spmv(sol, np.zeros_like(b), 1.0, 0.0), b) < 1e-9
 
 
 @pytest.mark.parametrize("mixed", [False, True])
