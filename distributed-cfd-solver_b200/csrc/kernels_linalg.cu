@@ -131,17 +131,17 @@ __global__ void __launch_bounds__(kLuThreads) k_lu(BsrView A, const MT* __restri
         }
         pv[k] = static_cast<int8_t>(m);
         if (mx == 0.0) ok = false;
-        if (m != k) {
+        // row swap by selects (no data-dependent branch, so a[] stays in
+        // registers)
 #pragma unroll
-            for (int r = k + 1; r < BS; ++r)
-                if (r == m) {
+        for (int r = k + 1; r < BS; ++r) {
+            const bool sw = (r == m);
 #pragma unroll
-                    for (int j = 0; j < BS; ++j) {
-                        const double tmp = a[k * BS + j];
-                        a[k * BS + j] = a[r * BS + j];
-                        a[r * BS + j] = tmp;
-                    }
-                }
+            for (int j = 0; j < BS; ++j) {
+                const double ak = a[k * BS + j], ar = a[r * BS + j];
+                a[k * BS + j] = sw ? ar : ak;
+                a[r * BS + j] = sw ? ak : ar;
+            }
         }
         const double inv_d = 1.0 / a[k * BS + k];
 #pragma unroll
@@ -163,12 +163,12 @@ __global__ void __launch_bounds__(kLuThreads) k_lu(BsrView A, const MT* __restri
 #pragma unroll
                 for (int k = 0; k < BS; ++k) {
 #pragma unroll
-                    for (int j = k + 1; j < BS; ++j)
-                        if (j == pv[k]) {
-                            const double t = x[k];
-                            x[k] = x[j];
-                            x[j] = t;
-                        }
+                    for (int j = k + 1; j < BS; ++j) {
+                        const bool sw = (j == pv[k]);
+                        const double xk = x[k], xj = x[j];
+                        x[k] = sw ? xj : xk;
+                        x[j] = sw ? xk : xj;
+                    }
                 }
 #pragma unroll
                 for (int r = 1; r < BS; ++r)
