@@ -136,9 +136,9 @@ def _case(cb, name: str, precision: str, scale: int = 1):
 
 
 # DRAM bytes (read + write) per algorithmic byte of a kernel family, from an
-# ncu capture of the same kernel on the 1/8-size plate, scaled to a full
-# launch by the rows it processes (profiles/sgs_rows_plate_scale2.md).
-TRAFFIC_PER_ALG_BYTE = {"sgs": 108.9 / 100.2}
+# ncu capture of the same kernels on the 1/8-size plate, scaled to a full
+# launch by the rows it processes (profiles/kernels_plate_scale2_fp64.md).
+TRAFFIC_PER_ALG_BYTE = {"sgs": 262.8 / 236.8, "spmv": 103.1 / 102.0}
 
 
 def _roofline(prof: dict, peak: float, peak_kind: str):

@@ -31,8 +31,14 @@ struct DevMesh {
     const double *ccx, *ccy, *ccz, *vol;        // n
     const int32_t *c2f_off, *c2f;        // cell -> faces (ascending)
     const int32_t *c2c_off, *c2c;        // cell -> face neighbours (sorted)
-    const int32_t *g_off, *g_col;        // gradient stencil
-    const double *g_wx, *g_wy, *g_wz;    // LSQ coefficients per stencil entry
+    // Gradient stencil in warp slices: cells 32s..32s+31 form slice s; its
+    // entries occupy slots [g_soff[s], g_soff[s+1]) with entry k of the cell
+    // in lane l at slot g_soff[s] + 32 k + l, each cell's entries in stencil
+    // order and padded to the slice's longest stencil with (own cell, zero
+    // weights), so a warp reads every entry array coalesced.
+    const int64_t* g_soff;               // ceil(n/32) + 1
+    const int32_t* g_col;                // slots
+    const double *g_wx, *g_wy, *g_wz;    // LSQ coefficients per slot
     const BcPatch* patches;
     int32_t n_patches;
     const double* wall_dist;             // n (SA)

@@ -94,7 +94,7 @@ constexpr int kLuThreads = 128;
 // (A x = e_c column by column), which is stored instead of the factors; the
 // multicolour sweep then applies D^-1 as a block-row product.
 template <typename MT, int BS, bool INV>
-__global__ void __launch_bounds__(kLuThreads) k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu,
+__global__ void __launch_bounds__(kLuThreads, 6) k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu,
                                                    int8_t* __restrict__ piv, int* __restrict__ err) {
     constexpr int B2 = BS * BS;
     __shared__ MT sm[kLuThreads * B2];

@@ -51,19 +51,23 @@ __global__ void k_primitives(DevMesh m, DevFields f, GasParams g) {
 template <int NVG>
 __global__ void __launch_bounds__(128) k_gradient(DevMesh m, const double* __restrict__ src, double* __restrict__ dst) {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.n) return;
+    const int32_t slice = c >> 5;
+    if (int64_t(slice) * 32 >= m.n) return;  // whole warps only
+    const bool act = c < m.n;
+    const int lane = threadIdx.x & 31;
     const int64_t nt = m.nt;
+    const int32_t cc = act ? c : m.n - 1;
     double qc[NVG], gx[NVG], gy[NVG], gz[NVG];
 #pragma unroll
     for (int v = 0; v < NVG; ++v) {
-        qc[v] = src[v * nt + c];
+        qc[v] = src[v * nt + cc];
         gx[v] = 0.0;
         gy[v] = 0.0;
         gz[v] = 0.0;
     }
-    const int32_t j1 = m.g_off[c + 1];
+    const int64_t s0 = m.g_soff[slice] + lane, s1 = m.g_soff[slice + 1];
 #pragma unroll 4
-    for (int32_t j = m.g_off[c]; j < j1; ++j) {
+    for (int64_t j = s0; j < s1; j += 32) {
         const int32_t nb = m.g_col[j];
         const double wx = m.g_wx[j], wy = m.g_wy[j], wz = m.g_wz[j];
 #pragma unroll
@@ -74,6 +78,7 @@ __global__ void __launch_bounds__(128) k_gradient(DevMesh m, const double* __res
             gz[v] += wz * d;
         }
     }
+    if (!act) return;
 #pragma unroll
     for (int v = 0; v < NVG; ++v) {
         dst[(v * 3 + 0) * nt + c] = gx[v];
@@ -152,7 +157,7 @@ __global__ void __launch_bounds__(128) k_limiter_ghostgrad(DevMesh m, DevFields 
 // (ResidualKernel::compute_fluxes, residual_kernel.hpp:175-306), and stores
 // F (5) and A*s_max (+ viscous radius) for the cell gather.
 template <bool MUSCL, bool VISC>
-__global__ void __launch_bounds__(128) k_face_flux(DevMesh m, DevFields f, GasParams g) {
+__global__ void __launch_bounds__(128, VISC ? 0 : 6) k_face_flux(DevMesh m, DevFields f, GasParams g) {
     const int32_t fc = blockIdx.x * blockDim.x + threadIdx.x;
     if (fc >= m.nf) return;
     const int64_t nt = m.nt, nf = m.nf;

@@ -744,7 +744,7 @@ Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, c
     sys_->set_profiler(&prof_);
     {
         const Csr c2f = build_cell_faces(hm);
-        const int64_t E = need_grad_ ? static_cast<int64_t>(g_col_.count) : 0;
+        const int64_t E = need_grad_ ? g_entries_ : 0;
         compute_alg_bytes(E, static_cast<int64_t>(c2c.val.size()), static_cast<int64_t>(c2f.val.size()));
     }
     if (sa_) setup_sa(hm);
@@ -820,11 +820,43 @@ void Solver::setup_mesh(const cfdg_mesh_host& mesh) {
         const Csr st = (cfg_.gradient == CFDG_GRAD_LSQ_FACE) ? c2c : build_cell_cells_node(hm);
         std::vector<double> wx, wy, wz;
         lsq_coefficients(hm, st, wx, wy, wz);
-        upload_or_throw(g_off_, st.off, s, "g_off");
-        upload_or_throw(g_col_, st.val, s, "g_col");
-        upload_or_throw(g_wx_, wx, s, "g_wx");
-        upload_or_throw(g_wy_, wy, s, "g_wy");
-        upload_or_throw(g_wz_, wz, s, "g_wz");
+        // warp slices (see DevMesh::g_soff)
+        const int32_t n = hm.n_cells;
+        const int32_t ns = (n + 31) / 32;
+        std::vector<int64_t> soff(static_cast<std::size_t>(ns) + 1, 0);
+        for (int32_t sl = 0; sl < ns; ++sl) {
+            int32_t len = 0;
+            for (int32_t c = sl * 32; c < std::min(n, sl * 32 + 32); ++c) len = std::max(len, st.off[c + 1] - st.off[c]);
+            soff[sl + 1] = soff[sl] + int64_t(len) * 32;
+        }
+        const std::size_t slots = static_cast<std::size_t>(soff[ns]);
+        std::vector<int32_t> scol(slots);
+        std::vector<double> swx(slots, 0.0), swy(slots, 0.0), swz(slots, 0.0);
+        for (int32_t sl = 0; sl < ns; ++sl) {
+            const int32_t len = static_cast<int32_t>((soff[sl + 1] - soff[sl]) / 32);
+            for (int l = 0; l < 32; ++l) {
+                const int32_t c = sl * 32 + l;
+                const int32_t cc = c < n ? c : n - 1;  // lanes past the last cell read a real cell
+                for (int32_t k = 0; k < len; ++k) {
+                    const std::size_t q = static_cast<std::size_t>(soff[sl] + int64_t(k) * 32 + l);
+                    const int32_t j = (c < n) ? st.off[c] + k : -1;
+                    if (j >= 0 && j < st.off[c + 1]) {
+                        scol[q] = st.val[j];
+                        swx[q] = wx[j];
+                        swy[q] = wy[j];
+                        swz[q] = wz[j];
+                    } else {
+                        scol[q] = cc;  // padding: own cell, zero weights
+                    }
+                }
+            }
+        }
+        g_entries_ = static_cast<int64_t>(st.val.size());
+        upload_or_throw(g_soff_, soff, s, "g_soff");
+        upload_or_throw(g_col_, scol, s, "g_col");
+        upload_or_throw(g_wx_, swx, s, "g_wx");
+        upload_or_throw(g_wy_, swy, s, "g_wy");
+        upload_or_throw(g_wz_, swz, s, "g_wz");
         // the host vectors die at scope end: make the copies complete first
         cuda_check(cudaStreamSynchronize(s), "setup sync");
     }
@@ -851,7 +883,7 @@ void Solver::setup_mesh(const cfdg_mesh_host& mesh) {
     dm_.c2f = c2f_.p;
     dm_.c2c_off = c2c_off_.p;
     dm_.c2c = c2c_.p;
-    dm_.g_off = g_off_.p;
+    dm_.g_soff = g_soff_.p;
     dm_.g_col = g_col_.p;
     dm_.g_wx = g_wx_.p;
     dm_.g_wy = g_wy_.p;
