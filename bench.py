@@ -243,6 +243,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         pg = dist
     case = _case(cb, args.case, args.precision, args.scale)
+    case.cfg.krylov_loop = cb.KRYLOV_HOST_LOOP if args.krylov_loop == "host" else cb.KRYLOV_DEVICE_LOOP
     mesh = cb.HostMesh(case.spec)
     n = mesh.n_cells
     s = cb.Solver(mesh, case.cfg, case.bcs, device=local)
@@ -354,7 +355,8 @@ def run_ours(args):
                            "nnzb": s.nnzb, "precision": args.precision,
                            "sgs": "multicolour", "krylov": "BiCGSTAB rtol 1e-3 max 30",
                            "krylov_iterations_per_step": round(float(np.mean(kry_timed)), 2),
-                           "krylov_loop": "device (one graph launch per linear solve)",
+                           "krylov_loop": ("device (one graph launch per linear solve)" if args.krylov_loop == "device"
+                                           else "host (one launch sequence per iteration)"),
                            "cfl_schedule": "1->100 geometric over 50 iterations",
                            "iterations_timed": f"{args.warmup + 1}..{args.warmup + args.steps}",
                            "l2": "inputs larger than L2 (Jacobian 1.45 GB, fields 0.5 GB)",
@@ -463,6 +465,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8 runs")
     ap.add_argument("--converge-scale", type=int, default=2, help="bump mesh divisor of the time-to-1e-8 runs")
+    ap.add_argument("--krylov-loop", default="device", choices=["device", "host"],
+                    help="BiCGSTAB driver of the timed steps (host: one launch sequence per iteration, "
+                         "e.g. for a profiler that does not see kernels inside conditional graph nodes)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
