@@ -368,16 +368,19 @@ def run_ours(args):
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = _cpu_baseline(cb, case, mesh, args.cpu_steps)
         if not args.no_converge and world == 1:
-            line["time_to_1e8"] = _time_to_converge(cb, args.converge_scale)
+            line["time_to_1e8"] = _time_to_converge(cb, args.converge_scale, not args.no_cpu_baseline)
         print(json.dumps(line))
     s.close()
     if pg is not None:
         pg.destroy_process_group()
 
 
-def _time_to_converge(cb, scale: int):
+def _time_to_converge(cb, scale: int, cpu: bool = True):
     """Wall time of run_steady to a 1e-8 residual drop on the bump: FP64,
-    mixed, mixed + learned guess (network trained first on other flows)."""
+    mixed, mixed + learned guess (network trained first on other flows);
+    with `cpu`, the reference CPU solver's seconds per iteration on the same
+    mesh times the FP64 run's iteration count (same algorithm and CFL
+    schedule: an extrapolated time to 1e-8)."""
     t0 = time.perf_counter()
     ds = cb.Dataset(5, 6_000_000)
     collect = []
@@ -423,6 +426,23 @@ def _time_to_converge(cb, scale: int):
             float("%.3g" % (np.linalg.norm(fields[name][v] - ref[v]) / max(np.linalg.norm(ref[v]), 1e-300)))
             for v in (0, 1, 2, 4)]
     out["speedup_mixed_learned_vs_fp64"] = round(out["fp64"]["seconds"] / out["mixed_learned"]["seconds"], 3)
+    if cpu:
+        import __graft_entry__ as ge
+        refh, _ = ge.load_oracle()
+        if refh.available():
+            c = cb.cases.bump(scale=scale, iterations=4000, mixed=False)
+            ref = refh.RefSolver(mesh, c.cfg, c.bcs)
+            ref.set_state(cb.cases.freestream_state(c, mesh.n_cells))
+            ref.newton_step(cb.cases.cfl_at(c.cfg, 1))  # first iteration outside the sample
+            t_r = time.perf_counter()
+            for k in range(2):
+                ref.newton_step(cb.cases.cfl_at(c.cfg, k + 2))
+            spi = (time.perf_counter() - t_r) / 2
+            out["reference_cpu"] = {"seconds_per_iteration": round(spi, 3), "cores": 1,
+                                    "sample": "iterations 2-3 of the same mesh, single-threaded reference build",
+                                    "extrapolated_seconds": round(spi * out["fp64"]["iterations"], 1),
+                                    "speedup_mixed_learned_vs_reference": round(
+                                        spi * out["fp64"]["iterations"] / out["mixed_learned"]["seconds"], 1)}
     # the limiter freezes from states that differ by the linear solves'
     # rounding; given the FP64 run's frozen limiter, mixed + learned converges
     # to the FP64 run's discrete solution
