@@ -431,12 +431,13 @@ def _time_to_converge(cb, scale: int, cpu: bool = True):
         refh, _ = ge.load_oracle()
         if refh.available():
             c = cb.cases.bump(scale=scale, iterations=4000, mixed=False)
-            ref = refh.RefSolver(mesh, c.cfg, c.bcs)
-            ref.set_state(cb.cases.freestream_state(c, mesh.n_cells))
-            ref.newton_step(cb.cases.cfl_at(c.cfg, 1))  # first iteration outside the sample
+            rsol = refh.RefSolver(mesh, c.cfg, c.bcs)
+            rsol.set_state(cb.cases.freestream_state(c, mesh.n_cells))
+            rsol.newton_step(cb.cases.cfl_at(c.cfg, 1))  # first iteration outside the sample
             t_r = time.perf_counter()
             for k in range(2):
-                ref.newton_step(cb.cases.cfl_at(c.cfg, k + 2))
+                rsol.newton_step(cb.cases.cfl_at(c.cfg, k + 2))
+            del rsol
             spi = (time.perf_counter() - t_r) / 2
             out["reference_cpu"] = {"seconds_per_iteration": round(spi, 3), "cores": 1,
                                     "sample": "iterations 2-3 of the same mesh, single-threaded reference build",

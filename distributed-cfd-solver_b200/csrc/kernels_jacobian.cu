@@ -24,8 +24,14 @@ __device__ __forceinline__ MT to_mt(double x) { return static_cast<MT>(x); }
 // Stores the block each lane of the warp holds in `stage[lane]` to its BSR
 // slot: the warp walks its 32 lanes' blocks and writes one contiguous block
 // per step (coalesced), instead of 32 scattered stores per instruction.
+// Staged block row stride: BS*BS padded to an odd number of elements so
+// that the 32 lanes writing entry e of their own block hit distinct banks.
+template <int BS>
+__host__ __device__ constexpr int stage_stride() { return (BS * BS) % 2 == 0 ? BS * BS + 1 : BS * BS; }
+
 template <typename MT, int BS>
-__device__ __forceinline__ void warp_store_blocks(MT (*stage)[BS * BS], int32_t pos, bool valid, MT* vals) {
+__device__ __forceinline__ void warp_store_blocks(MT (*stage)[stage_stride<BS>()], int32_t pos, bool valid,
+                                                  MT* vals) {
     __syncwarp();
     const int lane = threadIdx.x & 31;
     for (int src = 0; src < 32; ++src) {
@@ -148,8 +154,8 @@ __device__ __forceinline__ double visc_entry(const ViscFace& v, const GasParams&
 
 template <typename MT, bool VISC, int BS, bool FULL>
 __global__ void __launch_bounds__(128, 4) k_jac_rows(DevMesh m, DevFields f, GasParams g, JacStructure js, MT* vals) {
-    __shared__ MT stage_all[4][32][BS * BS];
-    MT(*stage)[BS * BS] = stage_all[threadIdx.x >> 5];
+    __shared__ MT stage_all[4][32][stage_stride<BS>()];
+    MT(*stage)[stage_stride<BS>()] = stage_all[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = r < m.n;

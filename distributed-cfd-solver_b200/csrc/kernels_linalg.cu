@@ -97,12 +97,13 @@ template <typename MT, int BS, bool INV>
 __global__ void __launch_bounds__(kLuThreads, 6) k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu,
                                                    int8_t* __restrict__ piv, int* __restrict__ err) {
     constexpr int B2 = BS * BS;
-    __shared__ MT sm[kLuThreads * B2];
+    constexpr int SP = B2 % 2 == 0 ? B2 + 1 : B2;  // odd row stride: thread-per-row accesses hit distinct banks
+    __shared__ MT sm[kLuThreads * SP];
     const int32_t r0 = blockIdx.x * kLuThreads;
     const int32_t nrows = min(kLuThreads, A.n - r0);
     for (int q = threadIdx.x; q < nrows * B2; q += kLuThreads) {
         const int row = q / B2, e = q - row * B2;
-        sm[q] = vals[int64_t(A.diag[r0 + row]) * B2 + e];
+        sm[row * SP + e] = vals[int64_t(A.diag[r0 + row]) * B2 + e];
     }
     __syncthreads();
     const int32_t i = r0 + threadIdx.x;
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(kLuThreads, 6) k_lu(BsrView A, const MT* __res
     double a[BS * BS];
     if (act) {
 #pragma unroll
-        for (int e = 0; e < BS * BS; ++e) a[e] = static_cast<double>(sm[threadIdx.x * B2 + e]);
+        for (int e = 0; e < BS * BS; ++e) a[e] = static_cast<double>(sm[threadIdx.x * SP + e]);
     } else {
 #pragma unroll
         for (int e = 0; e < BS * BS; ++e) a[e] = (e % (BS + 1) == 0) ? 1.0 : 0.0;
@@ -181,11 +182,11 @@ __global__ void __launch_bounds__(kLuThreads, 6) k_lu(BsrView A, const MT* __res
                     x[r] = x[r] / a[r * BS + r];
                 }
 #pragma unroll
-                for (int r = 0; r < BS; ++r) sm[threadIdx.x * B2 + r * BS + c] = static_cast<MT>(x[r]);
+                for (int r = 0; r < BS; ++r) sm[threadIdx.x * SP + r * BS + c] = static_cast<MT>(x[r]);
             }
         } else {
 #pragma unroll
-            for (int e = 0; e < BS * BS; ++e) sm[threadIdx.x * B2 + e] = static_cast<MT>(a[e]);
+            for (int e = 0; e < BS * BS; ++e) sm[threadIdx.x * SP + e] = static_cast<MT>(a[e]);
         }
 #pragma unroll
         for (int k = 0; k < BS; ++k) piv[int64_t(i) * BS + k] = pv[k];
@@ -201,7 +202,10 @@ __global__ void __launch_bounds__(kLuThreads, 6) k_lu(BsrView A, const MT* __res
     }
     __syncthreads();
     MT* dst = lu + int64_t(r0) * B2;
-    for (int q = threadIdx.x; q < nrows * B2; q += kLuThreads) dst[q] = sm[q];
+    for (int q = threadIdx.x; q < nrows * B2; q += kLuThreads) {
+        const int row = q / B2, e = q - row * B2;
+        dst[q] = sm[row * SP + e];
+    }
 }
 
 // Pivoted forward/backward substitution of one block (lu_solve_block) in
