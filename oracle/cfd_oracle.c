@@ -49,6 +49,7 @@ struct oracle_solver {
     int32_t *rp, *cols, *diag;
     int64_t nnzb;
     double *U, *q, *grad, *phi, *res, *lam, *alpha, *vals;
+    int phi_frozen; /* limiter values kept from the last evaluation (cfdg_solver_freeze_limiter) */
     /* Spalart-Allmaras */
     int sa;
     double nu_inf, rhonu_inf;
@@ -1014,7 +1015,7 @@ static void residual(oracle_solver* s) {
             for (int p = 0; p < 3; ++p) s->gnu[(size_t)p * nt + g] = sg * s->gnu[(size_t)p * nt + c0];
         }
     }
-    if (s->muscl) {
+    if (s->muscl && !s->phi_frozen) {
         /* Muscl::compute_limiters (numerics/reconstruction/muscl.hpp:25-105) */
         const double k3 = s->cfg.venkat_k * s->cfg.venkat_k * s->cfg.venkat_k;
         for (int c = 0; c < n; ++c) {
@@ -1587,6 +1588,10 @@ int oracle_newton_step(oracle_solver* s, double cfl, double* l2, int* krylov) {
     free(du);
     return 0;
 }
+
+/* Keep (1) or recompute (0) the MUSCL limiter values at later evaluations:
+ * the library's cfdg_solver_freeze_limiter, which the reference lacks. */
+void oracle_freeze_limiter(oracle_solver* s, int frozen) { s->phi_frozen = frozen ? 1 : 0; }
 
 void oracle_sa_fields(const oracle_solver* s, double* dist, double* nu, double* mut, double* gnu) {
     if (!s->sa) return;

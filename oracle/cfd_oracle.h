@@ -42,6 +42,7 @@ int oracle_nvars(const oracle_solver* s);
 /* Spalart-Allmaras fields: wall distance (n), nu_tilde (n), eddy viscosity
  * (n_total), nu_tilde gradient (3 x n_total); no-op without the model. */
 void oracle_sa_fields(const oracle_solver* s, double* dist, double* nu, double* mut, double* gnu);
+void oracle_freeze_limiter(oracle_solver* s, int frozen);
 
 /* linear algebra on raw BSR arrays */
 void oracle_bsr_spmv(int n, int bs, const int32_t* rp, const int32_t* cols, const double* vals, const double* x,

@@ -1,0 +1,149 @@
+"""CPU study on the oracle (test infrastructure, not part of the library):
+the laminar plate's steady convergence with the Picard Jacobian (the
+reference's backward-Euler Newton: the linear operator is the first-order
+BSR matrix) against a Jacobian-free Newton-Krylov operator
+v -> alpha v + (R(U + eps v) - R(U)) / eps on the full residual, both
+right-preconditioned by SGS on the Picard matrix (oracle/cfd_oracle.c) and
+solved by BiCGSTAB.  It measures what limits the plate's convergence; the
+library itself has only the Picard path.
+
+Usage (from the repository root):
+  python oracle/jfnk_study.py --order second --method jfnk --iterations 600 \
+      --cfl-max 1000 --scale 8 --freeze 150
+
+--freeze k: freeze the MUSCL limiter at iteration k (the Jacobian-free
+product needs a differentiable residual) and switch the JFNK operator on
+from there; before it both methods are identical.  CFL: geometric ramp
+1 -> 100 over 50 iterations, then switched evolution relaxation
+CFL = 100 * (rel at the ramp's end / rel), capped at --cfl-max.
+Prints one JSON line: every iterations/15 iterations the monitor
+(max over mass, |momentum|, energy of L2 / running maximum), the CFL, the
+Krylov iterations since the last line and the last linear reduction.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+
+def bicgstab(op, prec, b, tol, maxit):
+    """Right-preconditioned BiCGSTAB (the reference's algorithm, without the
+    breakdown checks): returns (x, iterations, final |r| / |b|)."""
+    x = np.zeros_like(b)
+    r = b.copy()
+    r0 = r.copy()
+    p = r.copy()
+    bn = np.linalg.norm(b)
+    if bn == 0.0:
+        return x, 0, 0.0
+    rho = r0 @ r
+    for k in range(1, maxit + 1):
+        ph = prec(p)
+        v = op(ph)
+        alpha = rho / (r0 @ v)
+        s = r - alpha * v
+        sh = prec(s)
+        t = op(sh)
+        om = (t @ s) / (t @ t)
+        x += alpha * ph + om * sh
+        r = s - om * t
+        if np.linalg.norm(r) <= tol * bn:
+            return x, k, float(np.linalg.norm(r) / bn)
+        rn = r0 @ r
+        beta = (rn / rho) * (alpha / om)
+        rho = rn
+        p = r + beta * (p - om * v)
+    return x, maxit, float(np.linalg.norm(r) / bn)
+
+
+def run(order, method, iterations, cfl_max, scale, freeze, lin_tol=1e-2, lin_max=60):
+    import __graft_entry__ as ge
+    import port
+    cb = ge.load_package()
+    case = cb.cases.plate(scale=scale)
+    if order == "first":
+        case.cfg.reconstruction = 0
+    mesh = cb.HostMesh(case.spec)
+    ora = port.PortSolver(mesh, case.cfg, case.bcs)
+    n, nv = mesh.n_cells, 5
+    rp, cols = ora.structure()
+    U = np.asarray(cb.cases.freestream_state(case, n)).reshape(nv, n).copy()
+
+    def resid(Ux):
+        ora.set_state(Ux)
+        return ora.stages()["res"].reshape(nv, n)
+
+    hist, mx, kry, ref_mon, cfl = [], None, 0, None, 1.0
+    t0 = time.time()
+    for it in range(1, iterations + 1):
+        R = resid(U)
+        l2 = np.sqrt((R ** 2).sum(axis=1) / n)
+        mon = np.array([l2[0], np.sqrt((l2[1:4] ** 2).sum()), l2[4]])
+        mx = mon if mx is None else np.maximum(mx, mon)
+        rel = float((mon / mx).max())
+        if not np.isfinite(rel):
+            hist.append(["blowup", it])
+            break
+        if freeze and it == freeze:
+            ora.freeze_limiter(True)
+        if it <= 50:
+            cfl = min(cfl_max, 100.0 ** ((it - 1) / 49))
+            if it == 50:
+                ref_mon = rel
+        elif freeze and it <= freeze:
+            cfl = 100.0
+            ref_mon = rel
+        else:
+            cfl = min(cfl_max, 100.0 * max(1.0, ref_mon / rel))
+        alpha, vals = ora.jacobian(cfl)
+        jfnk = method == "jfnk" and (not freeze or it >= freeze)
+        b = -R.T.ravel()
+        prec = lambda v: port.sgs_apply(rp, cols, vals, 5, v)  # noqa: E731
+        if jfnk:
+            Un = np.linalg.norm(U)
+            diag = np.repeat(alpha, nv)
+
+            def op(v):
+                vn = np.linalg.norm(v)
+                if vn == 0.0:
+                    return np.zeros_like(v)
+                eps = 1.5e-8 * (1.0 + Un) / vn
+                return diag * v + (resid(U + eps * v.reshape(n, nv).T) - R).T.ravel() / eps
+            du, k, red = bicgstab(op, prec, b, lin_tol, lin_max)
+        else:
+            op = lambda v: port.bsr_spmv(rp, cols, vals, 5, v)  # noqa: E731
+            du, k, red = bicgstab(op, prec, b, 1e-3, 30)
+        kry += k
+        U = U + du.reshape(n, nv).T
+        if it % max(1, iterations // 15) == 0 or rel < 1e-8:
+            hist.append([it, float("%.3g" % rel), float("%.3g" % cfl), kry, float("%.2g" % red)])
+            kry = 0
+        if rel < 1e-8:
+            break
+    return {"order": order, "method": method, "cells": n, "cfl_max": cfl_max, "freeze": freeze,
+            "wall_s": round(time.time() - t0, 1), "hist": hist}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--order", choices=["first", "second"], default="second")
+    ap.add_argument("--method", choices=["picard", "jfnk"], default="jfnk")
+    ap.add_argument("--iterations", type=int, default=600)
+    ap.add_argument("--cfl-max", type=float, default=1000.0)
+    ap.add_argument("--scale", type=int, default=8)
+    ap.add_argument("--freeze", type=int, default=150)
+    a = ap.parse_args()
+    print(json.dumps(run(a.order, a.method, a.iterations, a.cfl_max, a.scale, a.freeze)))
+
+
+if __name__ == "__main__":
+    main()

@@ -43,6 +43,7 @@ def _lib():
         L.oracle_nvars.argtypes = [C.c_void_p]
         L.oracle_nvars.restype = C.c_int
         L.oracle_sa_fields.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+        L.oracle_freeze_limiter.argtypes = [C.c_void_p, C.c_int]
         L.oracle_bsr_spmv.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_double, C.c_double]
         L.oracle_sgs_apply.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_int]
         L.oracle_bicgstab.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, C.c_int, C.c_double, C.c_double, C.c_int,
@@ -121,6 +122,11 @@ class PortSolver:
         dist, nu, mut, gnu = np.zeros(n), np.zeros(n), np.zeros(nt), np.zeros(3 * nt)
         _lib().oracle_sa_fields(self._h, _d(dist), _d(nu), _d(mut), _d(gnu))
         return {"wall_dist": dist, "nu": nu, "mut": mut, "nu_grad": gnu}
+
+    def freeze_limiter(self, frozen=True):
+        """Keep the limiter values of the last evaluation (as the library's
+        cfdg_solver_freeze_limiter)."""
+        _lib().oracle_freeze_limiter(self._h, 1 if frozen else 0)
 
     def jacobian(self, cfl):
         alpha = np.zeros(self.n)

@@ -118,3 +118,21 @@ def test_oracle_krylov_edge_cases(port, refh):
     assert info["iterations"] == 0 and info["status"] == 0
     x, info = port.bicgstab(rp, cols, 2 * vals, bs, b, precond=0, max_it=0)
     assert info["status"] == 2
+
+
+def test_oracle_frozen_limiter(cb, port):
+    """The oracle's frozen limiter (the library's cfdg_solver_freeze_limiter):
+    after freezing, a new state keeps the old limiter values; unfrozen, they
+    are recomputed."""
+    case, mesh = _case(cb, "ramp")
+    s = port.PortSolver(mesh, case.cfg, case.bcs)
+    U0 = cb.cases.perturbed_state(case, mesh.n_cells)
+    s.set_state(U0)
+    phi0 = s.stages()["phi"]
+    assert phi0.min() < 1.0  # the perturbed ramp state is limited somewhere
+    U1 = np.asarray(U0).reshape(5, -1) * (1.0 + 0.02 * np.sin(np.arange(mesh.n_cells)))
+    s.freeze_limiter(True)
+    s.set_state(U1)
+    assert np.array_equal(s.stages()["phi"], phi0)
+    s.freeze_limiter(False)
+    assert not np.array_equal(s.stages()["phi"], phi0)
