@@ -17,7 +17,7 @@ from there; before it both methods are identical.  CFL: geometric ramp
 1 -> 100 over 50 iterations, then switched evolution relaxation
 CFL = 100 * (rel at the ramp's end / rel), capped at --cfl-max.
 Prints one JSON line: every iterations/15 iterations the monitor
-(max over mass, |momentum|, energy of L2 / running maximum), the CFL, the
+(max over mass, |momentum|, energy[, nu_tilde] of L2 / running maximum), the CFL, the
 Krylov iterations since the last line and the last linear reduction.
 """
 from __future__ import annotations
@@ -65,16 +65,16 @@ def bicgstab(op, prec, b, tol, maxit):
     return x, maxit, float(np.linalg.norm(r) / bn)
 
 
-def run(order, method, iterations, cfl_max, scale, freeze, lin_tol=1e-2, lin_max=60):
+def run(order, method, iterations, cfl_max, scale, freeze, lin_tol=1e-2, lin_max=60, case_name="plate"):
     import __graft_entry__ as ge
     import port
     cb = ge.load_package()
-    case = cb.cases.plate(scale=scale)
+    case = cb.cases.plate(scale=scale) if case_name == "plate" else cb.cases.sa_plate(scale=scale, mixed=False)
     if order == "first":
         case.cfg.reconstruction = 0
     mesh = cb.HostMesh(case.spec)
     ora = port.PortSolver(mesh, case.cfg, case.bcs)
-    n, nv = mesh.n_cells, 5
+    n, nv = mesh.n_cells, ora.nv
     rp, cols = ora.structure()
     U = np.asarray(cb.cases.freestream_state(case, n)).reshape(nv, n).copy()
 
@@ -87,7 +87,7 @@ def run(order, method, iterations, cfl_max, scale, freeze, lin_tol=1e-2, lin_max
     for it in range(1, iterations + 1):
         R = resid(U)
         l2 = np.sqrt((R ** 2).sum(axis=1) / n)
-        mon = np.array([l2[0], np.sqrt((l2[1:4] ** 2).sum()), l2[4]])
+        mon = np.array([l2[0], np.sqrt((l2[1:4] ** 2).sum()), l2[4]] + ([l2[5]] if nv == 6 else []))
         mx = mon if mx is None else np.maximum(mx, mon)
         rel = float((mon / mx).max())
         if not np.isfinite(rel):
@@ -107,7 +107,7 @@ def run(order, method, iterations, cfl_max, scale, freeze, lin_tol=1e-2, lin_max
         alpha, vals = ora.jacobian(cfl)
         jfnk = method == "jfnk" and (not freeze or it >= freeze)
         b = -R.T.ravel()
-        prec = lambda v: port.sgs_apply(rp, cols, vals, 5, v)  # noqa: E731
+        prec = lambda v: port.sgs_apply(rp, cols, vals, nv, v)  # noqa: E731
         if jfnk:
             Un = np.linalg.norm(U)
             diag = np.repeat(alpha, nv)
@@ -120,7 +120,7 @@ def run(order, method, iterations, cfl_max, scale, freeze, lin_tol=1e-2, lin_max
                 return diag * v + (resid(U + eps * v.reshape(n, nv).T) - R).T.ravel() / eps
             du, k, red = bicgstab(op, prec, b, lin_tol, lin_max)
         else:
-            op = lambda v: port.bsr_spmv(rp, cols, vals, 5, v)  # noqa: E731
+            op = lambda v: port.bsr_spmv(rp, cols, vals, nv, v)  # noqa: E731
             du, k, red = bicgstab(op, prec, b, 1e-3, 30)
         kry += k
         U = U + du.reshape(n, nv).T
@@ -129,12 +129,13 @@ def run(order, method, iterations, cfl_max, scale, freeze, lin_tol=1e-2, lin_max
             kry = 0
         if rel < 1e-8:
             break
-    return {"order": order, "method": method, "cells": n, "cfl_max": cfl_max, "freeze": freeze,
+    return {"case": case_name, "order": order, "method": method, "cells": n, "cfl_max": cfl_max, "freeze": freeze,
             "wall_s": round(time.time() - t0, 1), "hist": hist}
 
 
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--case", choices=["plate", "sa_plate"], default="plate")
     ap.add_argument("--order", choices=["first", "second"], default="second")
     ap.add_argument("--method", choices=["picard", "jfnk"], default="jfnk")
     ap.add_argument("--iterations", type=int, default=600)
@@ -142,7 +143,7 @@ def main():
     ap.add_argument("--scale", type=int, default=8)
     ap.add_argument("--freeze", type=int, default=150)
     a = ap.parse_args()
-    print(json.dumps(run(a.order, a.method, a.iterations, a.cfl_max, a.scale, a.freeze)))
+    print(json.dumps(run(a.order, a.method, a.iterations, a.cfl_max, a.scale, a.freeze, case_name=a.case)))
 
 
 if __name__ == "__main__":
