@@ -136,3 +136,45 @@ def test_oracle_frozen_limiter(cb, port):
     assert np.array_equal(s.stages()["phi"], phi0)
     s.freeze_limiter(False)
     assert not np.array_equal(s.stages()["phi"], phi0)
+
+
+def _plate_bc_variant(cb, variant):
+    """The 1/8 plate with one boundary condition swapped for a kind or mode
+    the benchmark cases do not use."""
+    case = cb.cases.plate(scale=8, jacobian=cb.JAC_REFERENCE)
+    case.cfg.sgs_ordering = cb.SGS_LEVEL
+    fs = case.extra
+    if variant == "isothermal_wall":
+        case.bcs[3] = cb.bc(3, cb.BC_NO_SLIP_WALL, t=310.0)
+    elif variant == "heat_flux_wall":
+        case.bcs[3] = cb.bc(3, cb.BC_NO_SLIP_WALL_HEAT_FLUX, tmp_grad=-40.0)
+    elif variant == "inlet_mach_angles":
+        case.bcs[0] = cb.bc(0, cb.BC_SUBSONIC_INLET, inflow_mode=cb.INFLOW_MACH_ANGLES, p=fs["p"], t=fs["T"],
+                            mach=fs["mach"], alpha_deg=2.0, beta_deg=0.0)
+    elif variant == "inlet_mach_direction":
+        case.bcs[0] = cb.bc(0, cb.BC_SUBSONIC_INLET, inflow_mode=cb.INFLOW_MACH_DIRECTION, p=fs["p"], t=fs["T"],
+                            mach=fs["mach"], direction=(0.99, 0.1, 0.0))
+    elif variant == "farfield_top":
+        case.bcs[2] = cb.bc(2, cb.BC_FARFIELD, p=fs["p"], t=fs["T"], velocity=(fs["u"], 0.0, 0.0))
+    return case
+
+
+@pytest.mark.parametrize("variant", ["isothermal_wall", "heat_flux_wall", "inlet_mach_angles",
+                                     "inlet_mach_direction", "farfield_top"])
+def test_oracle_boundary_variants_match_reference_build(cb, refh, port, variant):
+    """Every boundary-condition kind and inflow mode the library accepts,
+    beyond the benchmark cases' own: oracle stages and Newton iterates
+    against the reference build."""
+    case = _plate_bc_variant(cb, variant)
+    mesh = cb.HostMesh(case.spec)
+    U0 = cb.cases.perturbed_state(case, mesh.n_cells, seed=13)
+    r, p = refh.RefSolver(mesh, case.cfg, case.bcs), port.PortSolver(mesh, case.cfg, case.bcs)
+    r.set_state(U0)
+    p.set_state(U0)
+    sr, sp = r.stages(), p.stages()
+    nt = mesh.n_cells + mesh.n_faces - mesh.n_inner
+    assert rel_err(sp["q"], sr["q"], nt) < 1e-13
+    assert rel_err(sp["res"], sr["res"], mesh.n_cells) < 1e-11
+    for cfl in (2.0, 20.0):
+        assert rel_err(p.newton_step(cfl), r.newton_step(cfl)) < 1e-10
+        assert rel_err(p.get_state().ravel(), r.get_state().ravel(), mesh.n_cells) < 1e-10
