@@ -22,8 +22,9 @@ Prints one JSON line: every iterations/15 iterations the monitor
 Krylov iterations since the last line and the last linear reduction.  A
 Jacobian-free solve that does not reduce the linear residual is replaced by
 the Picard step of the same iteration (counted in `picard_fallbacks`); a
-Jacobian-free step is scaled so that density and energy change by at most
-20% in any cell, and rho nu~ is clipped at zero.
+Jacobian-free step is scaled so that density, energy and rho nu~ (against
+its value plus 1e-3 of its RMS) change by at most 20% in any cell, and
+rho nu~ is clipped at zero.
 """
 from __future__ import annotations
 
@@ -140,6 +141,9 @@ def run(order, method, iterations, cfl_max, scale, freeze, lin_tol=1e-2, lin_max
         dU = du.reshape(n, nv).T
         if jfnk:  # relax the step to change density and energy by at most 20%; rho nu~ stays >= 0
             worst = max(np.abs(dU[0] / U[0]).max(), np.abs(dU[4] / U[4]).max())
+            if nv == 6:
+                floor = 1e-3 * np.sqrt((U[5] ** 2).mean())
+                worst = max(worst, np.abs(dU[5] / (np.abs(U[5]) + floor)).max())
             dU = dU * min(1.0, 0.2 / max(worst, 1e-300))
         U = U + dU
         if nv == 6:
