@@ -1,30 +1,37 @@
 """Benchmark of the implicit hot path on B200: Mcell-iter/s of full Newton
-iterations (residual -> 5x5 BSR Jacobian -> BiCGSTAB + SGS -> update) on the
-laminar flat-plate workload (256x128x32 hex, 1,048,576 cells, FP64).
+iterations (residual -> 6x6 BSR Jacobian -> BiCGSTAB + SGS -> update) on the
+Spalart-Allmaras flat plate (384x192x56 hex, 4,128,768 cells), plain FP64
+for `value`, with mixed precision and mixed precision + learned initial
+guess measured on the same iterations beside it; and time to a 1e-8
+residual drop, FP64 vs mixed vs mixed + learned guess.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--case plate|ramp|bump] [--precision fp64|mixed]
+                  [--case sa_plate|plate|bump|ramp] [--scale S]
 
-One step = one nonlinear iteration over the whole mesh.  `value` is timed
-with CUDA events on the solver stream (inputs resident in HBM; the 1.45 GB
-Jacobian and the field arrays exceed the 126 MB L2, so no flush is needed);
-`e2e` repeats the steps through the C ABI with the state copied in from
-pinned host memory and copied back every step.  Under torchrun each rank
-runs an independent replica on its own GPU (no data-path collective): value
-is the sum over ranks of cells x steps divided by the maximum rank time.
+One step = one nonlinear iteration over the whole mesh at the operating
+point after the CFL ramp: every leg first runs the case's 50-iteration CFL
+ramp (CFL 1 -> 100; the limiter freezes at its end, and the iterations
+before the freeze use the FP64 matrix in every leg), untimed, then W warm-up
+and K timed iterations at CFL 100.  `value` is timed with CUDA events on
+the solver stream with the state resident in HBM (the 8.3 GB Jacobian and
+the fields exceed the 126 MB L2, so no flush is needed); `e2e` replays the
+same K iterations from the same state through the C ABI with the state
+copied in from pinned host memory and back out every step.  Under torchrun
+each rank runs an independent replica on its own GPU (no data-path
+collective); value is the sum over ranks of cells x steps over the maximum
+rank time, and the mixed / learned legs and the time-to-1e-8 runs are
+single-GPU only.
 
-The second half of the metric, time to a 1e-8 residual drop, is the
-`time_to_1e8` object (single GPU): the transonic Euler bump (M = 0.85; the
+time_to_1e8 (single GPU): the transonic Euler bump (M = 0.85; the
 160x80x80x6-tet mesh divided by --converge-scale per direction, 2 by
-default: 768,000 cells) run to a 1e-8 residual drop three ways: plain FP64,
-mixed precision (FP32 Jacobian / SGS / SpMV), and mixed precision with the
-learned initial guess.  The network is trained on the GPU first, by the
-library's own tcgen05 kernels, on samples the solver writes out while it
-converges the bump at M = 0.8 and 0.9 on a mesh twice as coarse; that
-training is timed separately and is not part of the time to solution.
+default: 768,000 cells) run to a 1e-8 residual drop as plain FP64, mixed
+precision and mixed precision with the learned initial guess, each its own
+run from the free stream; converged fields are compared with the FP64 run.
+The Spalart-Allmaras plate does not reach 1e-8 with the first-order Picard
+Jacobian (the reference's method), so its time-to-1e-8 is not measured.
 
-`--impl reference` times the reference solver's own CPU implementation
-(built from its sources, oracle/_ref) on the same workload and metric.
+`--impl reference` times the reference's CPU implementation on a bounded
+sample of the same workload (see run_reference).
 """
 from __future__ import annotations
 
@@ -131,17 +138,50 @@ def _case(cb, name: str, precision: str, scale: int = 1):
     else:
         case = cb.cases.bump(scale=scale, mixed=mixed)
     if scale != 1:
-        case.description += f" (cell counts divided by {scale}^3)"
+        case.description += f" (each dimension divided by {scale})"
     return case
 
 
-# DRAM bytes (read + write) per algorithmic byte of a kernel family, from an
-# ncu capture of the same kernels on the 1/8-size plate, scaled to a full
-# launch by the rows it processes (profiles/kernels_plate_scale2_fp64.md).
+def _cfl(cb, case, it):
+    return cb.cases.cfl_at(case.cfg, it)
+
+
+def _prepare(cb, solver, case):
+    """The case's CFL ramp from the free stream (iterations 1..R, limiter
+    frozen at R): the operating point every timed window starts from."""
+    R = max(case.cfg.cfl_ramp_iterations, case.cfg.limiter_freeze, 1)
+    for it in range(1, R + 1):
+        if it == case.cfg.limiter_freeze:
+            solver.freeze_limiter(True)
+        solver.newton_step(_cfl(cb, case, it))
+    return R
+
+
+def _config(case, n, faces, nnzb, args, world, kry=None):
+    """The workload description both arms print (the driver pairs the arms
+    by it)."""
+    R = max(case.cfg.cfl_ramp_iterations, case.cfg.limiter_freeze, 1)
+    return {"workload": case.description, "case": case.name, "cells": int(n), "faces": int(faces),
+            "nnzb": int(nnzb), "block": 6 if case.cfg.turbulence else 5, "precision": "fp64",
+            "sgs": "multicolour (GPU) / sequential (CPU reference)", "krylov": "BiCGSTAB rtol 1e-3 max 30",
+            "cfl_schedule": f"1->{case.cfg.cfl_max:g} geometric over {case.cfg.cfl_ramp_iterations} iterations, "
+                            f"limiter frozen at {case.cfg.limiter_freeze}",
+            "iterations_timed": f"{R + args.warmup + 1}..{R + args.warmup + args.steps}",
+            "l2": "inputs larger than L2 (Jacobian and fields, no flush)",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
+
+
+# DRAM bytes (read + write) per algorithmic byte of a kernel family from ncu
+# captures of the same kernels on smaller meshes, scaled to a full launch by
+# the rows it processes: 6x6 FP64 blocks on the SA plate divided by 2 per
+# direction (profiles/kernels_sa_plate_scale2_fp64.md), 5x5 on the laminar
+# plate divided by 2 (profiles/kernels_plate_scale2_fp64.md).
 TRAFFIC_PER_ALG_BYTE = {"sgs": 262.8 / 236.8, "spmv": 103.1 / 102.0}
+TRAFFIC_PER_ALG_BYTE_SA = {}
 
 
-def _roofline(prof: dict, peak: float, peak_kind: str):
+def _roofline(prof: dict, peak: float, peak_kind: str, traffic_table: dict | None = None):
+    table_ratio = TRAFFIC_PER_ALG_BYTE if traffic_table is None else traffic_table
     fams = {k: v for k, v in prof.items() if v["launches"] > 0}
     total = sum(v["ms"] for v in fams.values())
     dom = max(fams, key=lambda k: fams[k]["ms"])
@@ -150,68 +190,15 @@ def _roofline(prof: dict, peak: float, peak_kind: str):
     per_launch_bytes = d["bytes"] / d["launches"]
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
     table = {k: {"ms_per_step_share": round(v["ms"] / total, 4), "launches": v["launches"],
-                 "gbs": round(v["bytes"] / (v["ms"] * 1e-3) / 1e9, 1) if v["ms"] > 0 else None}
+                 "gbs": round(v["bytes"] / (v["ms"] * 1e-3) / 1e9, 1) if v["ms"] > 0 else None,
+                 "frac": round(v["bytes"] / (v["ms"] * 1e-3) / 1e9 / peak, 3) if v["ms"] > 0 else None}
              for k, v in sorted(fams.items(), key=lambda kv: -kv[1]["ms"])}
     return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+            "frac": round(achieved / peak, 4),
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
             "bytes_per_launch": per_launch_bytes, "avg_launch_ms": per_launch_ms,
-            "traffic": (round(per_launch_bytes * TRAFFIC_PER_ALG_BYTE[dom]) if dom in TRAFFIC_PER_ALG_BYTE else None),
+            "traffic": (round(per_launch_bytes * table_ratio[dom]) if dom in table_ratio else None),
             "families": table}
-
-
-def _cpu_baseline(cb, case, mesh, steps: int):
-    """The reference CPU solver on the same mesh for a bounded sample."""
-    import __graft_entry__ as ge
-    refh, port = ge.load_oracle()
-    if refh.available():
-        ref = refh.RefSolver(mesh, case.cfg, case.bcs)
-        ref.set_state(cb.cases.freestream_state(case, mesh.n_cells))
-        ref.newton_step(_cfl(case, 1))  # first iteration outside the sample
-        t0 = time.perf_counter()
-        for k in range(steps):
-            ref.newton_step(_cfl(case, k + 2))
-        dt = time.perf_counter() - t0
-        kind = "reference"
-    else:
-        t0 = time.perf_counter()
-        dt = port.time_newton_steps(mesh, case, steps)
-        kind = "port"
-    value = mesh.n_cells * steps / dt / 1e6
-    return {"value": round(value, 5), "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": f"{steps} Newton iterations of the {mesh.n_cells}-cell {case.name} mesh, single-threaded "
-                      f"(the reference solver has no threading; MPI is not available here)"}
-
-
-def run_reference(args):
-    world, rank, local = _dist()
-    if rank != 0:
-        return
-    import __graft_entry__ as ge
-    cb = ge.load_package()
-    refh, port = ge.load_oracle()
-    case = _case(cb, args.case, "fp64", args.scale)
-    mesh = cb.HostMesh(case.spec)
-    if not refh.available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcfdref.so was not built"}))
-        return
-    ref = refh.RefSolver(mesh, case.cfg, case.bcs)
-    ref.set_state(cb.cases.freestream_state(case, mesh.n_cells))
-    for k in range(args.warmup):
-        ref.newton_step(_cfl(case, k + 1))
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        ref.newton_step(_cfl(case, args.warmup + k + 1))
-    dt = time.perf_counter() - t0
-    value = mesh.n_cells * args.steps / dt / 1e6
-    line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": case.description, "cells": mesh.n_cells, "case": case.name,
-                       "parallelism": "single CPU core (reference solver, np=1)"},
-            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": 1, "kind": "reference",
-                             "sample": f"{args.steps} Newton iterations after {args.warmup} warm-up"},
-            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
 
 
 def max_over_ranks(ms: float, dist_mod, device: str) -> float:
@@ -230,6 +217,163 @@ def replica_throughput(world: int, cells: int, steps: int, t_max_ms: float) -> f
     return world * cells * steps / (t_max_ms * 1e-3) / 1e6
 
 
+# ------------------------------------------------------------------ CPU side
+def _cpu_sample(case_name: str, scale: int, warmup: int, steps: int, step_cb=None):
+    """The reference's CPU implementation on a bounded sample of the
+    workload: the same case with each mesh dimension divided by `scale`,
+    built by the reference's own preprocessing (oracle refh.RefMesh), run
+    through the case's CFL ramp to the same operating point, then `warmup`
+    and `steps` timed Newton iterations.  The reference solver is used where
+    the reference has the physics (Euler, laminar Navier-Stokes); its
+    Spalart-Allmaras module does not compile (a header it includes is not in
+    the repository), so the turbulent case runs the oracle's C restatement
+    of it.  Single-threaded: the reference solver has no threading and its
+    only parallelism, MPI domain decomposition, is not available here.
+    Returns (seconds per step list, description, kind, mesh cells)."""
+    import __graft_entry__ as ge
+    cb = ge.load_package()  # configurations only: the product library is not loaded
+    refh, port = ge.load_oracle()
+    case = _case(cb, case_name, "fp64", scale)
+    mesh = refh.RefMesh(case.spec)
+    if case.cfg.turbulence:
+        solver, kind = port.PortSolver(mesh, case.cfg, case.bcs), "port"
+    else:
+        solver, kind = refh.RefSolver(mesh, case.cfg, case.bcs), "reference"
+    solver.set_state(cb.cases.freestream_state(case, mesh.n_cells))
+    R = _prepare(cb, solver, case)
+    it = R
+    for _ in range(warmup):
+        it += 1
+        solver.newton_step(_cfl(cb, case, it))
+    times = []
+    for _ in range(steps):
+        it += 1
+        t0 = time.perf_counter()
+        solver.newton_step(_cfl(cb, case, it))
+        times.append(time.perf_counter() - t0)
+        if step_cb:
+            step_cb(times[-1])
+    desc = (f"iterations {R + warmup + 1}..{R + warmup + steps} (after the CFL ramp) of the same case on its mesh "
+            f"divided by {scale} per direction ({mesh.n_cells} cells, built by the reference's preprocessing), "
+            f"{'the C restatement of the reference solver with the Spalart-Allmaras terms' if kind == 'port' else 'the reference solver built from its sources'}, "
+            f"one core")
+    return times, desc, kind, mesh.n_cells
+
+
+def run_reference(args):
+    """The reference arm: no product library is loaded.  Each step is one
+    Newton iteration of the bounded sample (_cpu_sample: the workload's
+    case at 1/`ref_scale` per direction, CFL ramp to the same operating
+    point); Mcell-iter/s is intensive, so the sample's rate stands for the
+    workload's."""
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    import __graft_entry__ as ge
+    refh, port = ge.load_oracle()
+    if not refh.available() or not port.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref libraries were not built"}))
+        return
+    cb = ge.load_package()
+    times, desc, kind, n_sample = _cpu_sample(args.case, args.ref_scale * args.scale, args.warmup, args.steps)
+    dt = float(sum(times))
+    value = n_sample * args.steps / dt / 1e6
+    case = _case(cb, args.case, "fp64", args.scale)
+    cells, faces, nnzb = _workload_sizes(cb, case)
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _config(case, cells, faces, nnzb, args, world),
+            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": 1, "kind": kind, "sample": desc},
+            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def _workload_sizes(cb, case):
+    """Cells, faces and BSR blocks of a case without building its mesh:
+    hex blocks have n = nx ny nz cells, 2(nx ny + ny nz + nx nz) boundary
+    faces and (6n - boundary) / 2 interior faces; the tet meshes split each
+    hex into 6 (4 faces per cell, two triangles per boundary quad); one
+    block row per cell plus two blocks per interior face."""
+    s = case.spec
+    nx, ny, nz = s.nx, s.ny, s.nz
+    fb = 2 * (nx * ny + ny * nz + nx * nz)
+    if s.kind == 2:
+        n = 6 * nx * ny * nz
+        fb *= 2
+        fi = (4 * n - fb) // 2
+    else:
+        n = nx * ny * nz
+        fi = (6 * n - fb) // 2
+    return n, fi + fb, n + 2 * fi
+
+
+# ------------------------------------------------------------------ GPU side
+def _train_sa_network(cb, device):
+    """The learned guess for the SA plate, trained on the GPU by the
+    library's own tcgen05 kernels on (features, dU) samples the solver writes
+    while running the training flows (cases.sa_training_flows: SA on the
+    laminar plate's mesh over M x Re_L); untimed."""
+    t0 = time.perf_counter()
+    flows = cb.cases.sa_training_flows()
+    ds = cb.Dataset(6, 3_000_000, device=device)
+    runs = []
+    for case in flows:
+        mesh = cb.HostMesh(case.spec)
+        stride = max(1, (mesh.n_cells * case.iterations) // 300_000)
+        with cb.Solver(mesh, case.cfg, case.bcs, device=device) as s:
+            s.init_fields()
+            s.attach_dataset(ds, stride)
+            r = s.run_steady()
+        runs.append({"mach": round(case.extra["mach"], 3), "Re": case.extra["Re"], "iterations": int(r.iterations)})
+    t_collect = time.perf_counter() - t0
+    net = cb.Mlp(6, seed=5, device=device)
+    t1 = time.perf_counter()
+    net.train(ds, epochs=40, batch=8192, lr=1e-3)
+    loss = net.train(ds, epochs=20, batch=8192, lr=2e-4)
+    info = {"samples": len(ds), "snapshots": sum(r["iterations"] for r in runs), "flows": len(runs),
+            "mesh": f"laminar plate mesh / 4 per direction ({cb.HostMesh(flows[0].spec).n_cells} cells)",
+            "epochs": "40 at lr 1e-3 + 20 at lr 2e-4", "final_loss": round(loss, 6),
+            "collect_s": round(t_collect, 2), "train_s": round(time.perf_counter() - t1, 3)}
+    ds.close()
+    return net, info
+
+
+def _timed_leg(cb, torch, s, case, stream, args, pg, local, it0, clocks=False):
+    """W warm-up and K timed Newton iterations from iteration it0; CUDA
+    events on the solver stream, barrier + synchronize on both sides."""
+    it = it0
+    kry = []
+    for _ in range(args.warmup):
+        it += 1
+        s.newton_step(_cfl(cb, case, it))
+    U_warm = s.get(cb.FIELD_U)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    launches0 = s.launch_count()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = Clocks(local) if clocks else None
+    if clk:
+        clk.__enter__()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        it += 1
+        kry.append(int(s.newton_step(_cfl(cb, case, it)).krylov_iterations))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__()
+    ms = ev0.elapsed_time(ev1)
+    barrier()
+    return {"ms": ms, "launches": s.launch_count() - launches0, "krylov": kry, "U_warm": U_warm,
+            "it_warm": it0 + args.warmup, "clocks": clk.summary() if clk else None}
+
+
 def run_ours(args):
     world, rank, local = _dist()
     import torch
@@ -242,145 +386,138 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         pg = dist
-    case = _case(cb, args.case, args.precision, args.scale)
+    case = _case(cb, args.case, "fp64", args.scale)
     case.cfg.krylov_loop = cb.KRYLOV_HOST_LOOP if args.krylov_loop == "host" else cb.KRYLOV_DEVICE_LOOP
+    t0 = time.perf_counter()
     mesh = cb.HostMesh(case.spec)
+    t_mesh = time.perf_counter() - t0
     n = mesh.n_cells
+    t0 = time.perf_counter()
     s = cb.Solver(mesh, case.cfg, case.bcs, device=local)
+    t_setup = time.perf_counter() - t0
     s.init_fields()
     stream = torch.cuda.ExternalStream(s.stream(), device=local)
-    it = 0
-    kry = []
+    R = _prepare(cb, s, case)
 
-    def step():
-        nonlocal it
-        it += 1
-        r = s.newton_step(float(_cfl(case, it)))
-        kry.append(int(r.krylov_iterations))
-        return r
-
-    for _ in range(args.warmup):
-        step()
-    # the state after warm-up: the profiled and end-to-end passes replay the
-    # timed iterations from it (same CFL schedule, same work)
-    U_warm = s.get(cb.FIELD_U)
-
-    def rewind():
-        nonlocal it
-        s.set_state(U_warm)
-        it = args.warmup
-
-    def barrier():
-        if pg is not None:
-            pg.barrier()
-        torch.cuda.synchronize()
-
-    # ---------------------------------------------------------- device-timed
-    # The product path: no profiler events, the Krylov iterations as one
-    # graph launch per linear solve.
-    launches0 = s.launch_count()
-    kry.clear()
-    barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            last = step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    launches = s.launch_count() - launches0
-    kry_timed = list(kry)
-    barrier()
-    t_max = max_over_ranks(ms, pg, f"cuda:{local}")
+    # ------------------------------------------------- FP64: the product path
+    leg = _timed_leg(cb, torch, s, case, stream, args, pg, local, R, clocks=True)
+    t_max = max_over_ranks(leg["ms"], pg, f"cuda:{local}")
     value = replica_throughput(world, n, args.steps, t_max)
+    U_warm, it_warm = leg["U_warm"], leg["it_warm"]
 
     # ------------------------------------------------- kernel-family events
-    # The timed iterations again, from the same state, with a CUDA event pair
+    # The timed iterations again from the same state with a CUDA event pair
     # around every kernel family on the solver's stream (the Krylov loop then
-    # runs host-driven so that each launch is bracketed); the roofline reads
-    # these durations.
-    rewind()
+    # runs host-driven so that each launch is bracketed).
+    s.set_state(U_warm)
     s.profile(True)
-    kry.clear()
+    kry_prof = []
     pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     pe0.record(stream)
-    for _ in range(args.steps):
-        step()
+    for k in range(args.steps):
+        kry_prof.append(int(s.newton_step(_cfl(cb, case, it_warm + k + 1)).krylov_iterations))
     pe1.record(stream)
     torch.cuda.synchronize()
     prof = s.profile_read()
     s.profile(False)
     prof_ms = pe0.elapsed_time(pe1)
-    kry_prof = list(kry)
-    barrier()
+    if pg is not None:
+        pg.barrier()
 
     # ---------------------------------------------------- end to end (C ABI)
-    # the first min(steps, 5) timed iterations once more, each with the
-    # state copied in from pinned host memory and the updated state read back
-    rewind()
+    # The same K iterations from the same state, each with the state copied
+    # in from pinned host memory and the updated state read back.
+    s.set_state(U_warm)
     U_host = torch.empty(s.field_size(cb.FIELD_U), dtype=torch.float64, pin_memory=True)
-    U_np = U_host.numpy()
-    U_np[:] = U_warm
+    U_host.numpy()[:] = U_warm
     import ctypes as C
     lib = cb.lib()
     ptr = C.cast(U_host.data_ptr(), C.POINTER(C.c_double))
-    e2e_steps = max(1, min(args.steps, 5))
-    barrier()
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(e2e_steps):
+    for k in range(args.steps):
         cb.check(lib.cfdg_solver_set_state(s._h, ptr, n))
-        step()
+        s.newton_step(_cfl(cb, case, it_warm + k + 1))
         cb.check(lib.cfdg_solver_get_field(s._h, cb.FIELD_U, ptr, U_host.numel()))
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    e2e_ms = max_over_ranks(e2e_ms, pg, f"cuda:{local}")
-    e2e_value = replica_throughput(world, n, e2e_steps, e2e_ms)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), pg, f"cuda:{local}")
+    e2e_value = replica_throughput(world, n, args.steps, e2e_ms)
     bytes_state = U_host.numel() * 8
+    nnzb, faces = s.nnzb, mesh.n_faces
+    s.close()
+
+    legs = {"fp64": {"value": round(value, 4), "ms_per_step": round(t_max / args.steps, 3),
+                     "krylov_iterations_per_step": round(float(np.mean(leg["krylov"])), 2)}}
+    if world == 1 and not args.no_mixed:
+        # mixed precision and mixed + learned guess: each its own run from the
+        # free stream (FP64 until the freeze), timed on the same iterations
+        net, train_info = (None, None)
+        if not args.no_learned:
+            net, train_info = _train_sa_network(cb, local) if case.cfg.turbulence else (None, None)
+        for name, learned in (("mixed", False), ("mixed_learned", True)):
+            if learned and net is None:
+                continue
+            c = _case(cb, args.case, "mixed", args.scale)
+            with cb.Solver(mesh, c.cfg, c.bcs, device=local) as sm:
+                sm.init_fields()
+                if learned:
+                    sm.attach_guess(net)
+                st = torch.cuda.ExternalStream(sm.stream(), device=local)
+                Rm = _prepare(cb, sm, c)
+                lg = _timed_leg(cb, torch, sm, c, st, args, None, local, Rm)
+                legs[name] = {"value": round(replica_throughput(1, n, args.steps, lg["ms"]), 4),
+                              "ms_per_step": round(lg["ms"] / args.steps, 3),
+                              "krylov_iterations_per_step": round(float(np.mean(lg["krylov"])), 2)}
+        if train_info:
+            legs["mixed_learned"]["training"] = train_info
+        if net is not None:
+            net.close()
 
     if rank == 0:
         peak, peak_kind = _peaks()
-        roof = _roofline(prof, peak, peak_kind)
-        roof["measured_in"] = (f"the timed iterations {args.warmup + 1}..{args.warmup + args.steps} replayed from the "
-                               f"same state with CUDA events around each kernel family and a host-driven Krylov "
-                               f"loop ({prof_ms / args.steps:.3f} ms per step, "
-                               f"{float(np.mean(kry_prof)):.2f} Krylov iterations per step)")
+        roof = _roofline(prof, peak, peak_kind, TRAFFIC_PER_ALG_BYTE_SA if case.cfg.turbulence else None)
+        roof["measured_in"] = (f"iterations {it_warm + 1}..{it_warm + args.steps} replayed from the same state with "
+                               f"CUDA events around each kernel family and a host-driven Krylov loop "
+                               f"({prof_ms / args.steps:.3f} ms per step, {float(np.mean(kry_prof)):.2f} Krylov "
+                               f"iterations per step)")
+        sizes = _workload_sizes(cb, case)
+        assert sizes == (n, faces, nnzb), (sizes, (n, faces, nnzb))
+        cfg_out = _config(case, n, faces, nnzb, args, world)
         line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(t_max / args.steps, 3), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-                "data": "synthetic",
-                "config": {"workload": case.description, "case": case.name, "cells": n, "faces": mesh.n_faces,
-                           "nnzb": s.nnzb, "precision": args.precision,
-                           "sgs": "multicolour", "krylov": "BiCGSTAB rtol 1e-3 max 30",
-                           "krylov_iterations_per_step": round(float(np.mean(kry_timed)), 2),
-                           "krylov_loop": ("device (one graph launch per linear solve)" if args.krylov_loop == "device"
-                                           else "host (one launch sequence per iteration)"),
-                           "cfl_schedule": "1->100 geometric over 50 iterations",
-                           "iterations_timed": f"{args.warmup + 1}..{args.warmup + args.steps}",
-                           "l2": "inputs larger than L2 (Jacobian 1.45 GB, fields 0.5 GB)",
-                           "parallelism": "replicas" if world > 1 else "single GPU"},
-                "clocks": clk.summary(), "gpu_launches": int(launches),
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": cfg_out, "clocks": leg["clocks"], "gpu_launches": int(leg["launches"]),
+                "krylov_iterations_per_step": legs["fp64"]["krylov_iterations_per_step"],
+                "legs": legs,
                 "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": bytes_state,
-                        "d2h_bytes_per_step": bytes_state, "steps": e2e_steps},
-                "roofline": roof}
+                        "d2h_bytes_per_step": bytes_state, "steps": args.steps,
+                        "iterations": f"{it_warm + 1}..{it_warm + args.steps}"},
+                "roofline": roof,
+                "setup_s": {"mesh": round(t_mesh, 2), "solver": round(t_setup, 2)}}
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = _cpu_baseline(cb, case, mesh, args.cpu_steps)
+            times, desc, kind, n_s = _cpu_sample(args.case, args.cpu_scale * args.scale, 1, args.cpu_steps)
+            v = n_s * len(times) / sum(times) / 1e6
+            line["cpu_baseline"] = {"value": round(v, 5), "unit": UNIT, "cores": 1, "kind": kind, "sample": desc}
         if not args.no_converge and world == 1:
             line["time_to_1e8"] = _time_to_converge(cb, args.converge_scale, not args.no_cpu_baseline)
         print(json.dumps(line))
-    s.close()
     if pg is not None:
         pg.destroy_process_group()
 
 
 def _time_to_converge(cb, scale: int, cpu: bool = True):
     """Wall time of run_steady to a 1e-8 residual drop on the bump: FP64,
-    mixed, mixed + learned guess (network trained first on other flows);
-    with `cpu`, the reference CPU solver's seconds per iteration on the same
-    mesh times the FP64 run's iteration count (same algorithm and CFL
-    schedule: an extrapolated time to 1e-8)."""
+    mixed, mixed + learned guess (network trained first on other flows),
+    each its own run from the free stream; the limiter freezes at the end of
+    the CFL ramp and the mixed runs use the FP64 matrix until then, so all
+    three solve the same frozen problem and their converged fields are
+    compared directly.  With `cpu`, the reference CPU solver's seconds per
+    iteration on the same mesh times the FP64 run's iteration count (same
+    algorithm and schedule: an extrapolated time to 1e-8)."""
     t0 = time.perf_counter()
     ds = cb.Dataset(5, 6_000_000)
     collect = []
@@ -401,14 +538,15 @@ def _time_to_converge(cb, scale: int, cpu: bool = True):
     net.train(ds, epochs=40, batch=8192, lr=1e-3)
     loss = net.train(ds, epochs=20, batch=8192, lr=2e-4)
     t_train = time.perf_counter() - t1
+    ds.close()
     case = cb.cases.bump(scale=scale, iterations=4000)
     mesh = cb.HostMesh(case.spec)
     out = {"workload": f"transonic Euler bump M=0.85, {mesh.n_cells} tets (160x80x80x6 / {scale}^3), "
                        f"run_steady to a 1e-8 drop of max(mass, |momentum|, energy) L2 vs its running maximum",
-           "training": {"samples": len(ds), "epochs": "40 at lr 1e-3 + 20 at lr 2e-4", "final_loss": round(loss, 6),
-                        "collect_s": round(t_collect, 2), "train_s": round(t_train, 3), "runs": collect}}
+           "training": {"samples": 6_000_000 if t_collect else 0, "epochs": "40 at lr 1e-3 + 20 at lr 2e-4",
+                        "final_loss": round(loss, 6), "collect_s": round(t_collect, 2), "train_s": round(t_train, 3),
+                        "runs": collect}}
     fields = {}
-    phi_fp64 = None
     for name, prec, learned in (("fp64", 0, False), ("mixed", 1, False), ("mixed_learned", 1, True)):
         c = cb.cases.bump(scale=scale, iterations=4000)
         c.cfg.precision = prec
@@ -418,15 +556,15 @@ def _time_to_converge(cb, scale: int, cpu: bool = True):
                 s.attach_guess(net)
             r = s.run_steady()
             fields[name] = s.get(cb.FIELD_U).reshape(5, -1)
-            if name == "fp64":
-                phi_fp64 = s.get(cb.FIELD_PHI)
         out[name] = {"seconds": round(r.seconds, 3), "iterations": int(r.iterations), "converged": bool(r.converged),
                      "rel": float(r.rel), "krylov_iterations": int(r.krylov_iterations_total)}
+    net.close()
     ref = fields["fp64"]
     for name in ("mixed", "mixed_learned"):
         out[name]["field_rel_l2_vs_fp64"] = [
             float("%.3g" % (np.linalg.norm(fields[name][v] - ref[v]) / max(np.linalg.norm(ref[v]), 1e-300)))
             for v in (0, 1, 2, 4)]
+    out["field_components"] = "rho, rho u, rho v, rho E"
     out["speedup_mixed_learned_vs_fp64"] = round(out["fp64"]["seconds"] / out["mixed_learned"]["seconds"], 3)
     if cpu:
         import __graft_entry__ as ge
@@ -446,33 +584,7 @@ def _time_to_converge(cb, scale: int, cpu: bool = True):
                                     "extrapolated_seconds": round(spi * out["fp64"]["iterations"], 1),
                                     "speedup_mixed_learned_vs_reference": round(
                                         spi * out["fp64"]["iterations"] / out["mixed_learned"]["seconds"], 1)}
-    # the limiter freezes from states that differ by the linear solves'
-    # rounding; given the FP64 run's frozen limiter, mixed + learned converges
-    # to the FP64 run's discrete solution
-    c = cb.cases.bump(scale=scale, iterations=4000)
-    c.cfg.precision = 1
-    with cb.Solver(mesh, c.cfg, c.bcs) as s:
-        s.init_fields()
-        s.attach_guess(net)
-        mx, it = None, 0
-        for it in range(1, 4001):
-            if it == c.cfg.limiter_freeze:
-                s.set_limiter(phi_fp64)
-            l2 = np.array(s.newton_step(cb.cases.cfl_at(c.cfg, it)).l2[:5])
-            mon = np.array([l2[0], np.sqrt((l2[1:4] ** 2).sum()), l2[4]])
-            mx = mon if mx is None else np.maximum(mx, mon)
-            if it > 1 and (mon / mx).max() <= c.cfg.residual_tolerance:
-                break
-        U = s.get(cb.FIELD_U).reshape(5, -1)
-    out["mixed_learned"]["same_limiter_iterations"] = it
-    out["mixed_learned"]["field_rel_l2_vs_fp64_same_limiter"] = [
-        float("%.3g" % (np.linalg.norm(U[v] - ref[v]) / max(np.linalg.norm(ref[v]), 1e-300))) for v in (0, 1, 2, 4)]
     return out
-
-
-def _cfl(case, it):
-    import __graft_entry__ as ge
-    return ge.load_package().cases.cfl_at(case.cfg, it)
 
 
 def main():
@@ -481,11 +593,15 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--case", default="plate", choices=["plate", "ramp", "bump", "sa_plate"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--case", default="sa_plate", choices=["sa_plate", "plate", "ramp", "bump"])
     ap.add_argument("--scale", type=int, default=1, help="divide each mesh dimension (profiling runs)")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--ref-scale", type=int, default=4,
+                    help="mesh divisor per direction of the reference arm's bounded sample")
+    ap.add_argument("--cpu-scale", type=int, default=8, help="mesh divisor of the cpu_baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed and mixed + learned legs")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-guess leg")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8 runs")
     ap.add_argument("--converge-scale", type=int, default=2, help="bump mesh divisor of the time-to-1e-8 runs")
     ap.add_argument("--krylov-loop", default="device", choices=["device", "host"],

@@ -46,6 +46,7 @@ KRYLOV_CONVERGED, KRYLOV_DIVERGED, KRYLOV_MAX_ITERATIONS = 0, 1, 2
  FIELD_MUT, FIELD_WALLDIST, FIELD_RHS, FIELD_NU, FIELD_NU_GRAD) = range(15)
 JAC_REFERENCE, JAC_THIN_LAYER = 0, 1
 KRYLOV_DEVICE_LOOP, KRYLOV_HOST_LOOP = 0, 1
+PREFREEZE_CONFIGURED, PREFREEZE_FP64 = 0, 1
 STAGE_PRIMITIVES, STAGE_GRADIENT, STAGE_LIMITER, STAGE_FLUXES = range(4)
 KCAT_NAMES = ("primitives", "gradient", "limiter", "face_flux", "cell_gather", "jacobian", "lu", "spmv", "sgs",
               "krylov", "update", "turbulence", "guess")
@@ -83,7 +84,8 @@ class Config(C.Structure):
                 ("precond", C.c_int32), ("sgs_ordering", C.c_int32), ("sgs_sweeps", C.c_int32),
                 ("lin_max_iterations", C.c_int32), ("cfl_ramp_iterations", C.c_int32),
                 ("residual_interval", C.c_int32), ("convergence_monitor", C.c_int32), ("jacobian", C.c_int32),
-                ("limiter_freeze", C.c_int32), ("krylov_loop", C.c_int32),
+                ("limiter_freeze", C.c_int32), ("krylov_loop", C.c_int32), ("pre_freeze", C.c_int32),
+                ("reserved_", C.c_int32),
                 ("gamma", C.c_double), ("gas_constant", C.c_double), ("prandtl", C.c_double),
                 ("prandtl_turb", C.c_double), ("init_rho", C.c_double), ("init_p", C.c_double),
                 ("init_velocity", C.c_double * 3), ("venkat_k", C.c_double), ("cfl", C.c_double),
@@ -220,10 +222,23 @@ def device_count() -> int:
     return n.value
 
 
+# cfdg_config_default's values (SolverConfig / SolverParams defaults of the
+# reference, include/cfd/solver/compressible/config.hpp:94-136 and
+# linalg/config.hpp:14-26), kept here so that configurations can be written
+# without loading the library (tests/test_abi_cpu.py checks the two agree).
+CONFIG_DEFAULTS = dict(
+    viscous=0, turbulence=0, gradient=GRAD_LSQ_NODE, reconstruction=RECON_MUSCL, limiter=LIM_VENKATAKRISHNAN,
+    precision=PREC_FP64, precond=PC_SGS, sgs_ordering=SGS_COLOR, sgs_sweeps=1, lin_max_iterations=500,
+    cfl_ramp_iterations=0, residual_interval=1, convergence_monitor=0, jacobian=JAC_REFERENCE, limiter_freeze=0,
+    krylov_loop=KRYLOV_DEVICE_LOOP, pre_freeze=PREFREEZE_CONFIGURED, reserved_=0,
+    gamma=1.4, gas_constant=287.052874, prandtl=0.71, prandtl_turb=0.9, init_rho=1.225, init_p=101325.0,
+    init_velocity=(0.0, 0.0, 0.0), venkat_k=0.5, cfl=0.4, cfl_max=0.4, residual_tolerance=1.0e-10,
+    lin_rel_tol=1.0e-1, lin_abs_tol=1.0e-15, nu_inf_ratio=3.0, max_iterations=10000)
+
+
 def default_config(**overrides) -> Config:
     cfg = Config()
-    lib().cfdg_config_default(C.byref(cfg))
-    for k, v in overrides.items():
+    for k, v in {**CONFIG_DEFAULTS, **overrides}.items():
         if k == "init_velocity":
             for i in range(3):
                 cfg.init_velocity[i] = v[i]

@@ -22,12 +22,21 @@ from dataclasses import dataclass, field
 from . import (BC_FARFIELD, BC_NO_SLIP_WALL_HEAT_FLUX, BC_SLIP_WALL, BC_SUBSONIC_INLET, BC_SUBSONIC_OUTLET,
                BC_SUPERSONIC_INLET, BC_SUPERSONIC_OUTLET, BC_SYMMETRY, GRAD_LSQ_NODE, JAC_THIN_LAYER,
                LIM_VENKATAKRISHNAN,
-               PC_SGS, PREC_FP64, RECON_MUSCL, SGS_COLOR, MeshSpec, bc, default_config)
+               PC_SGS, PREC_FP64, PREFREEZE_FP64, RECON_MUSCL, SGS_COLOR, MeshSpec, bc, default_config)
 
 GAMMA = 1.4
-# run_steady freezes the MUSCL limiter from this iteration on: the limiter's
-# on/off switching otherwise holds the residual at a plateau (1e-3 .. 1e-4)
-LIMITER_FREEZE = 300
+# run_steady freezes the MUSCL limiter from this iteration on, the last of
+# the 50-iteration CFL ramp: the limiter's on/off switching otherwise holds
+# the residual at a plateau (1e-3 .. 1e-4).  Switching also amplifies
+# round-off: two FP64 codes that differ only in their rounding (the
+# reference build and its C restatement) drift apart by 3e-8 after 100
+# iterations and 1.5e-6 after 300 on the ramp, and each converges to the
+# problem its own frozen limiter defines; frozen at the end of the ramp
+# they agree to 5e-11 and converge in 279 iterations instead of 464.
+LIMITER_FREEZE = 50
+# mixed precision and the learned guess start at the freeze (the iterates
+# before it are the FP64 path's): every precision solves one frozen problem
+PRE_FREEZE = PREFREEZE_FP64
 R_GAS = 287.052874
 
 
@@ -74,7 +83,7 @@ def ramp(scale: int = 1, seed: int = 1234, iterations: int = 200) -> Case:
                          venkat_k=0.5, precond=PC_SGS, sgs_ordering=SGS_COLOR, precision=PREC_FP64,
                          lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
                          cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
-                         limiter_freeze=LIMITER_FREEZE,
+                         limiter_freeze=LIMITER_FREEZE, pre_freeze=PRE_FREEZE,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))
     bcs = [bc(0, BC_SUPERSONIC_INLET, p=p, t=T, velocity=(u, 0.0, 0.0)),
            bc(1, BC_SUPERSONIC_OUTLET), bc(2, BC_SUPERSONIC_OUTLET), bc(3, BC_SLIP_WALL), bc(4, BC_SYMMETRY)]
@@ -101,7 +110,7 @@ def plate(scale: int = 1, seed: int = 4321, iterations: int = 200, mixed: bool =
                          precision=PREC_FP64 if not mixed else 1, prandtl=0.72, jacobian=jacobian,
                          lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
                          cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
-                         limiter_freeze=LIMITER_FREEZE,
+                         limiter_freeze=LIMITER_FREEZE, pre_freeze=PRE_FREEZE,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))
     # top boundary: symmetry plane (a Riemann far field there switches between
     # its inflow and outflow branches where v ~ 0 and holds a limit cycle)
@@ -114,25 +123,28 @@ def plate(scale: int = 1, seed: int = 4321, iterations: int = 200, mixed: bool =
                 {"mach": M, "Re": Re, "T": T, "p": p, "rho": rho, "u": u})
 
 
-def sa_plate(scale: int = 1, seed: int = 2468, iterations: int = 200, mixed: bool = True) -> Case:
+def sa_plate(scale: int = 1, seed: int = 2468, iterations: int = 200, mixed: bool = True, mach: float = 0.2,
+             reynolds: float = 5.0e6, spec: MeshSpec | None = None) -> Case:
     """Spalart-Allmaras RANS flat plate, M=0.2, Re_L=5e6, free-stream
     nu_tilde/nu = 3 (384x192x56 hex, 4,128,768 cells); wall-normal growth 1.1
-    from 1e-6 L, capped at 0.01 L."""
+    from 1e-6 L, capped at 0.01 L.  `spec` replaces the mesh (the learned
+    guess's training flows run on the laminar plate's mesh)."""
     nx, ny, nz = max(384 // scale, 8), max(192 // scale, 8), max(56 // scale, 2)
-    T, M, Re, L = 288.15, 0.2, 5.0e6, 1.0
+    T, M, Re, L = 288.15, mach, reynolds, 1.0
     u = M * sound_speed(T)
     mu = sutherland(T)
     rho = Re * mu / (u * L)
     p = rho * R_GAS * T
-    spec = _spec(1, nx, ny, nz, 1.25 * L, 0.0, 0.1 * L, seed, first_spacing=1.0e-6 * L * scale,
-                 stretch=1.1 ** scale, cap_spacing=0.01 * L * scale, jitter=0.05, plate_x0=0.25 * L)
+    if spec is None:
+        spec = _spec(1, nx, ny, nz, 1.25 * L, 0.0, 0.1 * L, seed, first_spacing=1.0e-6 * L * scale,
+                     stretch=1.1 ** scale, cap_spacing=0.01 * L * scale, jitter=0.05, plate_x0=0.25 * L)
     cfg = default_config(viscous=1, turbulence=1, nu_inf_ratio=3.0, gradient=GRAD_LSQ_NODE,
                          reconstruction=RECON_MUSCL, limiter=LIM_VENKATAKRISHNAN, venkat_k=0.5, precond=PC_SGS,
                          sgs_ordering=SGS_COLOR, precision=1 if mixed else PREC_FP64, prandtl=0.72,
                          jacobian=JAC_THIN_LAYER,
                          lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=100.0,
                          cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
-                         limiter_freeze=LIMITER_FREEZE,
+                         limiter_freeze=LIMITER_FREEZE, pre_freeze=PRE_FREEZE,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))
     bcs = [bc(0, BC_SUBSONIC_INLET, p=p, t=T, velocity=(u, 0.0, 0.0)),
            bc(1, BC_SUBSONIC_OUTLET, p=p),
@@ -141,6 +153,18 @@ def sa_plate(scale: int = 1, seed: int = 2468, iterations: int = 200, mixed: boo
            bc(4, BC_SYMMETRY), bc(5, BC_SYMMETRY)]
     return Case("sa_plate", spec, cfg, bcs, iterations, "SA RANS flat plate M=0.2 Re_L=5e6, 384x192x56 hex",
                 {"mach": M, "Re": Re, "T": T, "p": p, "rho": rho, "u": u, "nu_inf": 3.0 * mu / rho})
+
+
+def sa_training_flows(scale: int = 4, iterations: int = 200) -> list[Case]:
+    """The learned guess's training flows for the SA plate: Spalart-Allmaras
+    on the laminar plate's mesh (256x128x32 hex divided by `scale` per
+    direction, wall spacing 1e-5 L, growth 1.08) at M in {0.15, 0.2, 0.3} and
+    Re_L in {1e6, 5e6, 1e7}, mixed precision.  The compression ramp's
+    supersonic Euler block has no wall for the turbulence model and is not
+    used."""
+    spec = plate(scale=scale).spec
+    return [sa_plate(iterations=iterations, mixed=True, mach=m, reynolds=re, spec=spec)
+            for m in (0.15, 0.2, 0.3) for re in (1.0e6, 5.0e6, 1.0e7)]
 
 
 def bump(scale: int = 1, seed: int = 777, iterations: int = 200, mixed: bool = True, mach: float = 0.85) -> Case:
@@ -157,7 +181,7 @@ def bump(scale: int = 1, seed: int = 777, iterations: int = 200, mixed: bool = T
                          precision=1 if mixed else PREC_FP64,
                          lin_rel_tol=1e-3, lin_abs_tol=1e-30, lin_max_iterations=30, cfl=1.0, cfl_max=50.0,
                          cfl_ramp_iterations=50, max_iterations=iterations, residual_tolerance=1e-8, convergence_monitor=1,
-                         limiter_freeze=LIMITER_FREEZE,
+                         limiter_freeze=LIMITER_FREEZE, pre_freeze=PRE_FREEZE,
                          init_rho=rho, init_p=p, init_velocity=(u, 0.0, 0.0))
     far = dict(p=p, t=T, velocity=(u, 0.0, 0.0))
     bcs = [bc(0, BC_FARFIELD, **far), bc(1, BC_FARFIELD, **far), bc(2, BC_FARFIELD, **far), bc(3, BC_SLIP_WALL),

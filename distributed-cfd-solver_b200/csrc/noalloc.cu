@@ -15,7 +15,9 @@
 // has to start at zero, but calls that overlap on the GPU (two streams, two
 // host threads) race on it.  The first call on a device looks up the
 // array's device address on that device; make that first call outside any
-// stream capture.
+// stream capture.  The address is cached for the process's lifetime, so a
+// cudaDeviceReset (which re-creates the primary context and reloads this
+// module) leaves it stale: do not call the entry point after one.
 #include <cuda_runtime.h>
 
 #include <mutex>

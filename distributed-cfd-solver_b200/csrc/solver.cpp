@@ -230,6 +230,24 @@ BsrSystem::~BsrSystem() {
     if (ks_host_) cudaFreeHost(ks_host_);
 }
 
+void BsrSystem::set_precision(int precision) {
+    if (precision != CFDG_PREC_FP64 && precision != CFDG_PREC_MIXED) throw Failure{CFDG_ERR_INVALID, "unknown precision"};
+    if (precision == precision_) return;
+    const std::size_t nv = static_cast<std::size_t>(nnzb_) * bs_ * bs_;
+    release_device_loop();  // the captured iteration launches precision-specific kernels
+    if (precision == CFDG_PREC_MIXED) {
+        vals64_.release();
+        lu64_.release();
+        alloc_or_throw(vals32_, nv, "values");
+    } else {
+        vals32_.release();
+        lu32_.release();
+        alloc_or_throw(vals64_, nv, "values");
+    }
+    precision_ = precision;
+    lu_ready_ = false;
+}
+
 void BsrSystem::set_values_host(const double* v) {
     const std::size_t nv = static_cast<std::size_t>(nnzb_) * bs_ * bs_;
     if (precision_ == CFDG_PREC_MIXED) {
@@ -524,7 +542,7 @@ void BsrSystem::sgs_apply(const double* r, double* z, const int* active) {
 // capture or instantiation error leaves the host loop in charge.
 template <typename F>
 bool BsrSystem::device_loop_ready(int precond, double* x, const double* b, F&& iteration) {
-    const LoopKey key{precond, x, b, ordering_, sweeps_};
+    const LoopKey key{precond, x, b, ordering_, sweeps_, precision_};
     if (loop_exec_ && key == loop_key_) return true;
     if (loop_failed_) return false;
     release_device_loop();
@@ -714,6 +732,8 @@ Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, c
         throw Failure{CFDG_ERR_INVALID, "unknown Jacobian variant"};
     if (cfg.krylov_loop != CFDG_KRYLOV_DEVICE_LOOP && cfg.krylov_loop != CFDG_KRYLOV_HOST_LOOP)
         throw Failure{CFDG_ERR_INVALID, "unknown Krylov loop driver"};
+    if (cfg.pre_freeze != CFDG_PREFREEZE_CONFIGURED && cfg.pre_freeze != CFDG_PREFREEZE_FP64)
+        throw Failure{CFDG_ERR_INVALID, "unknown pre-freeze mode"};
     muscl_ = cfg.reconstruction == CFDG_RECON_MUSCL;
     need_grad_ = muscl_ || cfg.viscous;
     if (cfg.gradient != CFDG_GRAD_LSQ_FACE && cfg.gradient != CFDG_GRAD_LSQ_NODE && need_grad_)
@@ -1060,7 +1080,8 @@ void Solver::setup_matrix(const HostMesh& hm, const Csr& c2c) {
         std::sort(cols.begin() + s0, cols.end());
         row_ptr[r + 1] = static_cast<int32_t>(cols.size());
     }
-    sys_ = std::make_unique<BsrSystem>(device_, n, nv_, row_ptr.data(), cols.data(), cfg_.precision, stream_);
+    sys_ = std::make_unique<BsrSystem>(device_, n, nv_, row_ptr.data(), cols.data(),
+                                       pre_freeze_phase() ? CFDG_PREC_FP64 : cfg_.precision, stream_);
     sys_->device_loop = cfg_.krylov_loop == CFDG_KRYLOV_DEVICE_LOOP;
     auto pos = [&](int32_t row, int32_t col) -> int32_t {
         const auto b = cols.begin() + row_ptr[row], e = cols.begin() + row_ptr[row + 1];
@@ -1351,7 +1372,7 @@ void Solver::assemble_jacobian() {
     js.cell_of = row_of_h_.empty() ? nullptr : cell_of_.p;
     {
         ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 1, ab_.jac);
-        if (cfg_.precision == CFDG_PREC_MIXED)
+        if (sys_->precision() == CFDG_PREC_MIXED)
             launch_jacobian<float>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values32(), stream_);
         else
             launch_jacobian<double>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values64(), stream_);
@@ -1361,10 +1382,12 @@ void Solver::assemble_jacobian() {
 
 cfdg_krylov_result Solver::linear_solve() {
     if (cfg_.precond == CFDG_PC_SGS) sys_->sgs_setup(cfg_.sgs_ordering, std::max(cfg_.sgs_sweeps, 1));
-    if (guess_ || dataset_) prepare_guess_inputs();
+    const bool prefix = pre_freeze_phase();
+    if ((guess_ && !prefix) || dataset_) prepare_guess_inputs();
     // the network predicts the update relative to the previous one: no
-    // guess before a previous update exists
-    const bool use_guess = guess_ && have_prev_;
+    // guess before a previous update exists (nor before the limiter freeze
+    // under CFDG_PREFREEZE_FP64)
+    const bool use_guess = guess_ && have_prev_ && !prefix;
     if (use_guess) {
         ProfScope ps(&prof_, CFDG_KCAT_GUESS, stream_, 1, double(dm_.n) * (kMlpIn * 2.0 + nv_ * 8.0));
         guess_->forward(feat_.p, dm_.n, gscale_.p + 8, du_.p, stream_);
@@ -1443,6 +1466,7 @@ void Solver::residual_norms(double* l2_host) {
 
 cfdg_step_result Solver::newton_step(double cfl) {
     cfdg_step_result r{};
+    sys_->set_precision(pre_freeze_phase() ? CFDG_PREC_FP64 : cfg_.precision);
     evaluate_residual();
     compute_dt(cfl);
     assemble_jacobian();

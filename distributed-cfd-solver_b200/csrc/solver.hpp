@@ -125,6 +125,10 @@ public:
     double* values64() { return vals64_.p; }
     float* values32() { return vals32_.p; }
 
+    // Switches the stored matrix precision (CFDG_PREC_*): values and block
+    // LU of the new precision are allocated, the other precision's released,
+    // and set-up must run again before the next apply.
+    void set_precision(int precision);
     void set_values_host(const double* v);
     void get_values_host(double* v);
     // y = alpha*A*x + beta*y (device vectors)
@@ -196,9 +200,10 @@ private:
         int precond = -1;
         const double* x = nullptr;
         const double* b = nullptr;
-        int ordering = -1, sweeps = 0;
+        int ordering = -1, sweeps = 0, precision = -1;
         bool operator==(const LoopKey& o) const {
-            return precond == o.precond && x == o.x && b == o.b && ordering == o.ordering && sweeps == o.sweeps;
+            return precond == o.precond && x == o.x && b == o.b && ordering == o.ordering && sweeps == o.sweeps &&
+                   precision == o.precision;
         }
     };
     LoopKey loop_key_;
@@ -238,6 +243,9 @@ public:
     void attach_guess(Mlp* m);
     void attach_dataset(Dataset* d, int32_t stride);
     void freeze_limiter(bool frozen) { limiter_frozen_ = frozen; }
+    // CFDG_PREFREEZE_FP64 and the limiter not yet frozen: FP64 matrix, zero
+    // initial guess
+    bool pre_freeze_phase() const { return cfg_.pre_freeze == CFDG_PREFREEZE_FP64 && !limiter_frozen_; }
     void set_limiter(const double* phi, int64_t count);
 
 private:

@@ -159,6 +159,16 @@ enum { CFDG_JAC_REFERENCE = 0, CFDG_JAC_THIN_LAYER = 1 };
 /* BiCGSTAB iteration driver (cfdg_config.krylov_loop). */
 enum { CFDG_KRYLOV_DEVICE_LOOP = 0, CFDG_KRYLOV_HOST_LOOP = 1 };
 
+/* Linear solves before the limiter freeze (cfdg_config.pre_freeze).
+ * CONFIGURED: the configured matrix precision and initial guess throughout.
+ * FP64: until the limiter is frozen the linear solves use the FP64 matrix
+ * and start from zero (no learned guess), so the iterates up to the freeze
+ * are bitwise those of the plain FP64 path, the frozen limiter is the same,
+ * and a mixed-precision / learned-guess run converges to the FP64 run's
+ * discrete solution (the switching limiter makes the state at the freeze,
+ * and with it the frozen problem, depend on every rounding before it). */
+enum { CFDG_PREFREEZE_CONFIGURED = 0, CFDG_PREFREEZE_FP64 = 1 };
+
 /* Solver configuration: SolverConfig + linalg::SolverParams
  * (include/cfd/solver/compressible/config.hpp:94-136, linalg/config.hpp:14-26)
  * plus the CFL ramp, precision, SGS ordering, SA and learned-guess options. */
@@ -191,6 +201,8 @@ typedef struct cfdg_config {
      * the host loop); CFDG_KRYLOV_HOST_LOOP: one launch sequence per
      * iteration with the host reading the state after each. */
     int32_t krylov_loop;
+    int32_t pre_freeze;       /* CFDG_PREFREEZE_*                             */
+    int32_t reserved_;        /* zero                                         */
     double gamma, gas_constant, prandtl, prandtl_turb;
     double init_rho, init_p, init_velocity[3];
     double venkat_k;
@@ -310,7 +322,9 @@ CFDG_API int cfdg_residual_norms(cfdg_solver* s, double* l2_h);
  * NULL (legacy default stream); the call synchronises it.  Calls share the
  * scratch, so calls that overlap on the GPU race; the first call on a device
  * looks up the scratch address there and should come before any stream
- * capture. */
+ * capture.  The address is kept for the life of the process: after a
+ * cudaDeviceReset (or anything else that re-creates the device's primary
+ * context) the entry point must not be called again in that process. */
 CFDG_API int cfdg_residual_norms_noalloc(const double* res_d, int32_t n_cells, int32_t nvars, void* stream,
                                          double* l2_h);
 /* Solver::run_steady (solver.hpp:597-660) with the CFL ramp. */

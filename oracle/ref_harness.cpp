@@ -18,10 +18,13 @@
 #include <mpi.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <random>
+#include <string>
 #include <vector>
 
 #include "cfd/linalg/bicgstab.hpp"
@@ -29,8 +32,11 @@
 #include "cfd/linalg/preconditioners.hpp"
 #include "cfd/mesh/aux_connectivity.hpp"
 #include "cfd/mesh/aux_geometry.hpp"
+#include "cfd/mesh/faces.hpp"
 #include "cfd/mesh/geometry.hpp"
 #include "cfd/mesh/localmesh.hpp"
+#include "cfd/mesh/raw_mesh.hpp"
+#include "cfd/mesh/reorder.hpp"
 #include "cfd/mesh/validate.hpp"
 #include "cfd/numerics/gradient/gradient_manager.hpp"
 #include "cfd/numerics/limiter/slope_limiters.hpp"
@@ -181,6 +187,24 @@ sc::SolverConfig build_cfg(const cfdg_config& c) {
     return s;
 }
 
+// Limiter freeze through the reference's reconstruction-policy seam
+// (ReconstructionPolicy, include/cfd/numerics/reconstruction/concepts.hpp):
+// while g_limiter_frozen is set, compute_limiters leaves the Solver's phi
+// slots as last computed, which is what the GPU library's limiter freeze
+// does.  The reference itself recomputes phi on every residual evaluation.
+bool g_limiter_frozen = false;
+
+template <typename L>
+struct FreezableMuscl : numerics::recon::Muscl<L> {
+    template <std::size_t NVars>
+    static void compute_limiters(const mesh::MeshPart& mesh, const mesh::MeshAuxConnectivity& aux_conn,
+                                 const double* const* q, const double* const* gx, const double* const* gy,
+                                 const double* const* gz, double* const* phi, const double venkat_k = 1.0) noexcept {
+        if (!g_limiter_frozen)
+            numerics::recon::Muscl<L>::template compute_limiters<NVars>(mesh, aux_conn, q, gx, gy, gz, phi, venkat_k);
+    }
+};
+
 struct RefBase {
     virtual ~RefBase() = default;
     virtual void set_state(const double* U, int64_t ld) = 0;
@@ -189,6 +213,7 @@ struct RefBase {
     virtual void jacobian(double cfl, double* alpha, double* values) = 0;
     virtual int newton_step(double cfl, double* l2, int* kit, int* kstat, double* kinit, double* kfinal) = 0;
     virtual int64_t nnzb() const = 0;
+    bool frozen = false;
 };
 
 template <typename Phys, typename Recon>
@@ -323,7 +348,9 @@ struct RefImpl final : RefBase {
     // One BackwardEuler::advance through the reference Solver.
     int newton_step(double cfl, double* l2, int* kit, int* kstat, double* kinit, double* kfinal) override {
         const_cast<sc::SolverConfig&>(solver->config()).cfl = cfl;
+        g_limiter_frozen = frozen;
         time.advance(*solver);
+        g_limiter_frozen = false;
         // residual_norms (solver.hpp:740-756) of the R(U) evaluated this step
         auto rs = solver->res_slots();
         for (int v = 0; v < 5; ++v) {
@@ -410,16 +437,16 @@ REFH_API int refh_create(const cfdg_mesh_host* m, const cfdg_config* c, const cf
     if (c->reconstruction == CFDG_RECON_MUSCL) {
         switch (c->limiter) {
             case CFDG_LIM_BARTH_JESPERSEN:
-                if (visc) s->impl = std::make_unique<RefImpl<sc::physics::ViscousFlow, recon::Muscl<limiter::BarthJespersen>>>(std::move(mp), cfg, bcfg, c->venkat_k);
-                else s->impl = std::make_unique<RefImpl<sc::physics::InviscidFlow, recon::Muscl<limiter::BarthJespersen>>>(std::move(mp), cfg, bcfg, c->venkat_k);
+                if (visc) s->impl = std::make_unique<RefImpl<sc::physics::ViscousFlow, FreezableMuscl<limiter::BarthJespersen>>>(std::move(mp), cfg, bcfg, c->venkat_k);
+                else s->impl = std::make_unique<RefImpl<sc::physics::InviscidFlow, FreezableMuscl<limiter::BarthJespersen>>>(std::move(mp), cfg, bcfg, c->venkat_k);
                 break;
             case CFDG_LIM_VAN_ALBADA:
-                if (visc) s->impl = std::make_unique<RefImpl<sc::physics::ViscousFlow, recon::Muscl<limiter::VanAlbada>>>(std::move(mp), cfg, bcfg, c->venkat_k);
-                else s->impl = std::make_unique<RefImpl<sc::physics::InviscidFlow, recon::Muscl<limiter::VanAlbada>>>(std::move(mp), cfg, bcfg, c->venkat_k);
+                if (visc) s->impl = std::make_unique<RefImpl<sc::physics::ViscousFlow, FreezableMuscl<limiter::VanAlbada>>>(std::move(mp), cfg, bcfg, c->venkat_k);
+                else s->impl = std::make_unique<RefImpl<sc::physics::InviscidFlow, FreezableMuscl<limiter::VanAlbada>>>(std::move(mp), cfg, bcfg, c->venkat_k);
                 break;
             default:
-                if (visc) s->impl = std::make_unique<RefImpl<sc::physics::ViscousFlow, recon::Muscl<limiter::Venkatakrishnan>>>(std::move(mp), cfg, bcfg, c->venkat_k);
-                else s->impl = std::make_unique<RefImpl<sc::physics::InviscidFlow, recon::Muscl<limiter::Venkatakrishnan>>>(std::move(mp), cfg, bcfg, c->venkat_k);
+                if (visc) s->impl = std::make_unique<RefImpl<sc::physics::ViscousFlow, FreezableMuscl<limiter::Venkatakrishnan>>>(std::move(mp), cfg, bcfg, c->venkat_k);
+                else s->impl = std::make_unique<RefImpl<sc::physics::InviscidFlow, FreezableMuscl<limiter::Venkatakrishnan>>>(std::move(mp), cfg, bcfg, c->venkat_k);
                 break;
         }
     } else {
@@ -446,6 +473,11 @@ REFH_API int refh_stages(refh_solver* s, double* q, double* grad, double* phi, d
 }
 REFH_API int refh_jacobian(refh_solver* s, double cfl, double* alpha, double* values) {
     s->impl->jacobian(cfl, alpha, values);
+    return 0;
+}
+// Freezes (1) or releases (0) the limiter of the whole-iteration path.
+REFH_API int refh_freeze_limiter(refh_solver* s, int frozen) {
+    s->impl->frozen = frozen != 0;
     return 0;
 }
 REFH_API int refh_newton_step(refh_solver* s, double cfl, double* l2) {
@@ -517,3 +549,288 @@ REFH_API int refh_bicgstab(int n, int bs, const int32_t* row_ptr, const int32_t*
     *r_final = r.final_residual;
     return 0;
 }
+
+// ------------------------------------------------------------------ meshes
+// The benchmark meshes built through the reference's own preprocessing
+// pipeline, as apps/mesh_partition.cpp:198-405 runs it at one rank:
+// RawMesh (cells with CGNS node order, node coordinates, boundary surface
+// elements with their patch) -> mesh::build_faces (src/mesh/faces.cpp) ->
+// mesh::migrate_local_mesh with every cell on rank 0 (src/mesh/localmesh.cpp)
+// -> compute_mesh_geometry -> reorder_local_mesh(RCM) -> validate.
+// The node coordinates, cell connectivity, boundary patches and the seeded
+// cell shuffle restate the synthetic generator of the benchmark cases
+// (cfdg_mesh_spec: structured block, plate stretching with a cap, ramp and
+// circular-arc bump walls, seeded node jitter, Kuhn split into tetrahedra);
+// faces, their order, geometry and the RCM numbering are the reference's.
+namespace {
+
+struct Mt64 {
+    std::mt19937_64 g;
+    explicit Mt64(uint64_t s) : g(s) {}
+    double sym() { return 2.0 * (static_cast<double>(g() >> 11) * (1.0 / 9007199254740992.0)) - 1.0; }
+};
+
+struct RawGen {
+    std::vector<double> x, y, z;
+    std::vector<uint8_t> type;
+    std::vector<int32_t> off, nodes;
+    std::vector<std::array<int32_t, 4>> bface;  // boundary face nodes (-1 padded)
+    std::vector<int32_t> bpatch;
+    int n_patches = 0;
+};
+
+RawGen generate_raw(const cfdg_mesh_spec& s) {
+    RawGen r;
+    const int64_t NX = s.nx + 1, NY = s.ny + 1, NZ = s.nz + 1;
+    auto nid = [&](int64_t i, int64_t j, int64_t k) { return static_cast<int32_t>((k * NY + j) * NX + i); };
+    std::vector<double> xs(NX), ys(NY), zs(NZ);
+    for (int64_t i = 0; i < NX; ++i) xs[i] = s.lx * double(i) / double(s.nx);
+    for (int64_t k = 0; k < NZ; ++k) zs[k] = s.lz * double(k) / double(s.nz);
+    if (s.kind == 1) {
+        ys[0] = 0.0;
+        double h = s.first_spacing > 0 ? s.first_spacing : s.ly / s.ny;
+        for (int64_t j = 1; j < NY; ++j) {
+            ys[j] = ys[j - 1] + h;
+            double hn = h * (s.stretch > 0 ? s.stretch : 1.0);
+            if (s.cap_spacing > 0 && hn > s.cap_spacing) hn = s.cap_spacing;
+            h = hn;
+        }
+    } else {
+        for (int64_t j = 0; j < NY; ++j) ys[j] = s.ly * double(j) / double(s.ny);
+    }
+    auto wall = [&](double xv) {
+        if (s.kind == 0) return std::max(0.0, (xv - s.ramp_x) * std::tan(s.ramp_angle_deg * M_PI / 180.0));
+        if (s.kind == 2 && s.bump_height > 0 && xv > s.bump_x0 && xv < s.bump_x1) {
+            const double half = 0.5 * (s.bump_x1 - s.bump_x0), hh = s.bump_height * (s.bump_x1 - s.bump_x0);
+            const double R = (half * half + hh * hh) / (2.0 * hh), xm = 0.5 * (s.bump_x0 + s.bump_x1);
+            return std::sqrt(std::max(0.0, R * R - (xv - xm) * (xv - xm))) + (hh - R);
+        }
+        return 0.0;
+    };
+    const int64_t nn = NX * NY * NZ;
+    r.x.resize(nn);
+    r.y.resize(nn);
+    r.z.resize(nn);
+    for (int64_t k = 0; k < NZ; ++k)
+        for (int64_t j = 0; j < NY; ++j)
+            for (int64_t i = 0; i < NX; ++i) {
+                const int32_t n = nid(i, j, k);
+                r.x[n] = xs[i];
+                r.y[n] = s.kind == 1 ? ys[j] : wall(xs[i]) + (ys[j] / s.ly) * (s.ly - wall(xs[i]));
+                r.z[n] = zs[k];
+            }
+    if (s.jitter > 0) {
+        Mt64 rng(s.seed ^ 0x9e3779b97f4a7c15ULL);
+        const std::vector<double> x0(r.x), y0(r.y), z0(r.z);
+        if (s.kind == 1) {  // whole wall-normal lines in x/z, whole rows in y
+            for (int64_t k = 1; k < NZ - 1; ++k)
+                for (int64_t i = 1; i < NX - 1; ++i) {
+                    const double ox = s.jitter * std::min(xs[i + 1] - xs[i], xs[i] - xs[i - 1]) * rng.sym();
+                    const double oz = s.jitter * std::min(zs[k + 1] - zs[k], zs[k] - zs[k - 1]) * rng.sym();
+                    for (int64_t j = 0; j < NY; ++j) {
+                        r.x[nid(i, j, k)] = x0[nid(i, j, k)] + ox;
+                        r.z[nid(i, j, k)] = z0[nid(i, j, k)] + oz;
+                    }
+                }
+            for (int64_t j = 1; j < NY - 1; ++j) {
+                const double oy = s.jitter * std::min(ys[j + 1] - ys[j], ys[j] - ys[j - 1]) * rng.sym();
+                for (int64_t k = 0; k < NZ; ++k)
+                    for (int64_t i = 0; i < NX; ++i) r.y[nid(i, j, k)] = y0[nid(i, j, k)] + oy;
+            }
+        } else {  // every interior node by a fraction of its shortest edge
+            auto d = [&](int32_t a, int32_t b) {
+                return std::sqrt((x0[a] - x0[b]) * (x0[a] - x0[b]) + (y0[a] - y0[b]) * (y0[a] - y0[b]) +
+                                 (z0[a] - z0[b]) * (z0[a] - z0[b]));
+            };
+            for (int64_t k = 1; k < NZ - 1; ++k)
+                for (int64_t j = 1; j < NY - 1; ++j)
+                    for (int64_t i = 1; i < NX - 1; ++i) {
+                        const int32_t n = nid(i, j, k);
+                        const double h = std::min({d(n, nid(i + 1, j, k)), d(n, nid(i - 1, j, k)), d(n, nid(i, j + 1, k)),
+                                                   d(n, nid(i, j - 1, k)), d(n, nid(i, j, k + 1)), d(n, nid(i, j, k - 1))});
+                        r.x[n] = x0[n] + s.jitter * h * rng.sym();
+                        r.y[n] = y0[n] + s.jitter * h * rng.sym();
+                        r.z[n] = z0[n] + s.jitter * h * rng.sym();
+                    }
+        }
+    }
+    r.off.push_back(0);
+    for (int64_t k = 0; k < s.nz; ++k)
+        for (int64_t j = 0; j < s.ny; ++j)
+            for (int64_t i = 0; i < s.nx; ++i) {
+                const int32_t v[8] = {nid(i, j, k),     nid(i + 1, j, k),     nid(i + 1, j + 1, k),     nid(i, j + 1, k),
+                                      nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1), nid(i, j + 1, k + 1)};
+                if (s.kind != 2) {
+                    r.type.push_back(static_cast<uint8_t>(mesh::CellType::HEXA));
+                    r.nodes.insert(r.nodes.end(), v, v + 8);
+                    r.off.push_back(static_cast<int32_t>(r.nodes.size()));
+                    continue;
+                }
+                // six tetrahedra around the (0,0,0)-(1,1,1) diagonal, one per
+                // axis order; corners listed so that det[n1-n0,n2-n0,n3-n0] > 0
+                static const int ord[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+                for (const auto& o : ord) {
+                    int bits = 0, corner[4] = {0, 0, 0, 0};
+                    for (int q = 0; q < 3; ++q) corner[q + 1] = (bits |= 1 << o[q]);
+                    int32_t t[4];
+                    for (int q = 0; q < 4; ++q)
+                        t[q] = nid(i + (corner[q] & 1), j + ((corner[q] >> 1) & 1), k + ((corner[q] >> 2) & 1));
+                    double e[3][3];
+                    for (int q = 0; q < 3; ++q) {
+                        e[q][0] = r.x[t[q + 1]] - r.x[t[0]];
+                        e[q][1] = r.y[t[q + 1]] - r.y[t[0]];
+                        e[q][2] = r.z[t[q + 1]] - r.z[t[0]];
+                    }
+                    const double det = e[0][0] * (e[1][1] * e[2][2] - e[1][2] * e[2][1]) -
+                                       e[0][1] * (e[1][0] * e[2][2] - e[1][2] * e[2][0]) +
+                                       e[0][2] * (e[1][0] * e[2][1] - e[1][1] * e[2][0]);
+                    if (det < 0) std::swap(t[1], t[2]);
+                    r.type.push_back(static_cast<uint8_t>(mesh::CellType::TET));
+                    r.nodes.insert(r.nodes.end(), t, t + 4);
+                    r.off.push_back(static_cast<int32_t>(r.nodes.size()));
+                }
+            }
+    // boundary surface elements: cell faces whose nodes all lie on one
+    // boundary plane; patches ramp/bump 0 inlet 1 outlet 2 top 3 wall
+    // 4 z-planes; plate additionally 5 = lower symmetry ahead of plate_x0
+    r.n_patches = s.kind == 1 ? 6 : 5;
+    const std::size_t nc = r.type.size();
+    for (std::size_t c = 0; c < nc; ++c) {
+        const int ti = r.type[c];
+        for (int f = 0; f < mesh::kFacesPerType[ti]; ++f) {
+            const int fn = mesh::kFaceNodes[ti][f];
+            std::array<int32_t, 4> fnodes = {-1, -1, -1, -1};
+            bool i0 = true, iN = true, j0 = true, jN = true, k0 = true, kN = true;
+            double xc = 0.0;
+            for (int q = 0; q < fn; ++q) {
+                const int32_t n = r.nodes[r.off[c] + mesh::kFaceTable[ti][f][q]];
+                fnodes[q] = n;
+                const int64_t i = n % NX, j = (n / NX) % NY, k = n / (NX * NY);
+                i0 &= i == 0;
+                iN &= i == NX - 1;
+                j0 &= j == 0;
+                jN &= j == NY - 1;
+                k0 &= k == 0;
+                kN &= k == NZ - 1;
+                xc += xs[i] / fn;
+            }
+            int p = -1;
+            if (i0) p = 0;
+            else if (iN) p = 1;
+            else if (jN) p = 2;
+            else if (j0) p = (s.kind == 1 && xc < s.plate_x0) ? 5 : 3;
+            else if (k0 || kN) p = 4;
+            if (p < 0) continue;
+            r.bface.push_back(fnodes);
+            r.bpatch.push_back(p);
+        }
+    }
+    return r;
+}
+
+}  // namespace
+
+struct refh_mesh {
+    mesh::MeshPart mp;
+    cfdg_mesh_host view{};
+};
+
+REFH_API int refh_mesh_generate(const cfdg_mesh_spec* spec, refh_mesh** out) {
+    const cfdg_mesh_spec& s = *spec;
+    if (s.nx < 1 || s.ny < 1 || s.nz < 1 || s.kind < 0 || s.kind > 2) return -1;
+    RawGen g = generate_raw(s);
+    const int64_t nc = static_cast<int64_t>(g.type.size()), nn = static_cast<int64_t>(g.x.size());
+    // seeded shuffle of the cell numbering (Fisher-Yates), before the
+    // reference's own renumbering
+    std::vector<int32_t> order(nc);
+    for (int64_t c = 0; c < nc; ++c) order[c] = static_cast<int32_t>(c);
+    if (s.permute) {
+        Mt64 rng(s.seed);
+        for (int64_t i = nc - 1; i > 0; --i)
+            std::swap(order[i], order[static_cast<int64_t>(rng.g() % static_cast<uint64_t>(i + 1))]);
+    }
+    mesh::RawMesh raw;
+    raw.nprocs = 1;
+    raw.rank = 0;
+    raw.comm = MPI_COMM_WORLD;
+    raw.n_cells_g = nc;
+    raw.n_nodes_g = nn;
+    raw.cell_displ = {0, static_cast<GlobalIndex>(nc)};
+    raw.node_displ = {0, static_cast<GlobalIndex>(nn)};
+    raw.ctype.resize(nc);
+    raw.cnodes_offsets.assign(1, 0);
+    for (int64_t c = 0; c < nc; ++c) {
+        const int32_t o = order[c];
+        raw.ctype[c] = static_cast<mesh::CellType>(g.type[o]);
+        for (int32_t q = g.off[o]; q < g.off[o + 1]; ++q) raw.cnodes.push_back(g.nodes[q]);
+        raw.cnodes_offsets.push_back(static_cast<LocalIndex>(raw.cnodes.size()));
+    }
+    raw.my_node_coords_x = std::move(g.x);
+    raw.my_node_coords_y = std::move(g.y);
+    raw.my_node_coords_z = std::move(g.z);
+    raw.surf_elems.resize(g.bface.size());
+    for (std::size_t b = 0; b < g.bface.size(); ++b) {
+        mesh::SurfElem& e = raw.surf_elems[b];
+        int cnt = 0;
+        for (int q = 0; q < 4; ++q)
+            if (g.bface[b][q] >= 0) e.key.v[cnt++] = g.bface[b][q];
+        std::sort(e.key.v.begin(), e.key.v.begin() + cnt);
+        e.eid = static_cast<GlobalIndex>(b + 1);
+        e.patch = g.bpatch[b];
+    }
+    for (int p = 0; p < g.n_patches; ++p) {
+        mesh::BCMeta m;
+        m.name = "patch" + std::to_string(p);
+        m.cgns_type = "UserDefined";
+        raw.bcs.push_back(m);
+        raw.patch_list.emplace_back(m.name, m.cgns_type);
+    }
+    mesh::BuildFacesResult bf = mesh::build_faces(raw);
+    partition::PartitionResult pr;
+    pr.cell_target_rank.assign(static_cast<std::size_t>(nc), 0);
+    pr.part2rank = {0};
+    pr.rank2part = {0};
+    auto* m = new refh_mesh();
+    mesh::migrate_local_mesh(std::move(raw), std::move(bf.faces), pr, m->mp);
+    mesh::compute_mesh_geometry(m->mp);
+    if (s.reorder_rcm) mesh::reorder_local_mesh(m->mp, mesh::ReorderMethod::RCM);
+    mesh::validate_and_log_meshpart(m->mp);
+    mesh::MeshPart& mp = m->mp;
+    cfdg_mesh_host& v = m->view;
+    v.n_cells = mp.n_cells;
+    v.n_faces = mp.n_faces;
+    v.n_inner_faces = mp.n_inner_faces;
+    v.n_nodes = mp.n_nodes;
+    v.n_patches = static_cast<int32_t>(mp.patches.size());
+    v.cell_type = reinterpret_cast<const uint8_t*>(mp.cell_type.data());
+    v.cell_nodes_offsets = mp.cell_nodes_offsets.data();
+    v.cell_nodes = mp.cell_nodes.data();
+    v.node_x = mp.node_x.data();
+    v.node_y = mp.node_y.data();
+    v.node_z = mp.node_z.data();
+    v.cell_centroid_x = mp.cell_centroid_x.data();
+    v.cell_centroid_y = mp.cell_centroid_y.data();
+    v.cell_centroid_z = mp.cell_centroid_z.data();
+    v.cell_volume = mp.cell_volume.data();
+    v.face_owner = mp.face_owner.data();
+    v.face_neigh = mp.face_neigh.data();
+    v.face_patch = mp.face_patch.data();
+    v.face_nodes_offsets = mp.face_nodes_offsets.data();
+    v.face_nodes = mp.face_nodes.data();
+    v.face_centroid_x = mp.face_centroid_x.data();
+    v.face_centroid_y = mp.face_centroid_y.data();
+    v.face_centroid_z = mp.face_centroid_z.data();
+    v.face_normal_x = mp.face_normal_x.data();
+    v.face_normal_y = mp.face_normal_y.data();
+    v.face_normal_z = mp.face_normal_z.data();
+    v.face_area = mp.face_area.data();
+    *out = m;
+    return 0;
+}
+
+REFH_API int refh_mesh_view(const refh_mesh* m, cfdg_mesh_host* view) {
+    *view = m->view;
+    return 0;
+}
+
+REFH_API void refh_mesh_free(refh_mesh* m) { delete m; }

@@ -44,6 +44,10 @@ def _lib():
         L.refh_stages.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         L.refh_jacobian.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
         L.refh_newton_step.argtypes = [C.c_void_p, C.c_double, _dp]
+        L.refh_freeze_limiter.argtypes = [C.c_void_p, C.c_int]
+        L.refh_mesh_generate.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+        L.refh_mesh_view.argtypes = [C.c_void_p, C.c_void_p]
+        L.refh_mesh_free.argtypes = [C.c_void_p]
         L.refh_bsr_spmv.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_double, C.c_double]
         L.refh_sgs_apply.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_int]
         L.refh_bicgstab.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, C.c_int, C.c_double, C.c_double, C.c_int, _dp,
@@ -95,6 +99,63 @@ def wall_distance(mesh, wall_patches, max_sweeps=100000, rel_tol=0.0):
     return out
 
 
+_up = C.POINTER(C.c_uint8)
+
+
+class MeshHost(C.Structure):
+    """cfdg_mesh_host of include/cfdg.h (the view RefMesh hands out)."""
+    _fields_ = [("n_cells", C.c_int32), ("n_faces", C.c_int32), ("n_inner_faces", C.c_int32),
+                ("n_nodes", C.c_int32), ("n_patches", C.c_int32),
+                ("cell_type", _up), ("cell_nodes_offsets", _ip), ("cell_nodes", _ip),
+                ("node_x", _dp), ("node_y", _dp), ("node_z", _dp),
+                ("cell_centroid_x", _dp), ("cell_centroid_y", _dp), ("cell_centroid_z", _dp), ("cell_volume", _dp),
+                ("face_owner", _ip), ("face_neigh", _ip), ("face_patch", _ip),
+                ("face_nodes_offsets", _ip), ("face_nodes", _ip),
+                ("face_centroid_x", _dp), ("face_centroid_y", _dp), ("face_centroid_z", _dp),
+                ("face_normal_x", _dp), ("face_normal_y", _dp), ("face_normal_z", _dp), ("face_area", _dp)]
+
+
+class RefMesh:
+    """A benchmark mesh built by the reference's own preprocessing pipeline
+    (build_faces -> migrate_local_mesh at one rank -> compute_mesh_geometry
+    -> reorder_local_mesh(RCM) -> validate, as apps/mesh_partition.cpp runs
+    it) from the seeded synthetic generator's cells, nodes and boundary
+    patches.  Same interface as the product's HostMesh (`view`, `n_cells`,
+    `n_faces`, `n_inner`), so RefSolver and the C restatement take it."""
+
+    def __init__(self, spec):
+        h = C.c_void_p()
+        if _lib().refh_mesh_generate(C.byref(spec), C.byref(h)) != 0:
+            raise ValueError("invalid mesh spec")
+        self._h = h
+        self.spec = spec
+        self.view = MeshHost()
+        _lib().refh_mesh_view(self._h, C.byref(self.view))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().refh_mesh_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n_cells(self) -> int:
+        return self.view.n_cells
+
+    @property
+    def n_faces(self) -> int:
+        return self.view.n_faces
+
+    @property
+    def n_inner(self) -> int:
+        return self.view.n_inner_faces
+
+
 class RefSolver:
     """Reference solver over one mesh/config (5 mean-flow variables)."""
 
@@ -139,6 +200,11 @@ class RefSolver:
         vals = np.zeros(self.nnzb * 25)
         _lib().refh_jacobian(self._h, cfl, _d(alpha), _d(vals))
         return alpha, vals
+
+    def freeze_limiter(self, frozen=True):
+        """Keep the Solver's limiter values of the last evaluation (the
+        library's limiter freeze, applied through the reconstruction policy)."""
+        _lib().refh_freeze_limiter(self._h, 1 if frozen else 0)
 
     def newton_step(self, cfl):
         l2 = np.zeros(5)

@@ -42,6 +42,20 @@ def test_config_defaults_match_reference(cb):
     assert cfg.init_p == 101325.0 and cfg.init_rho == 1.225 and cfg.max_iterations == 10000
 
 
+def test_python_config_defaults_equal_library(cb):
+    # default_config() writes its values without loading the library; they
+    # must be cfdg_config_default's, field by field
+    lib_cfg = cb.Config()
+    cb.lib().cfdg_config_default(C.byref(lib_cfg))
+    py_cfg = cb.default_config()
+    for name, ctype in cb.Config._fields_:
+        a, b = getattr(lib_cfg, name), getattr(py_cfg, name)
+        if name == "init_velocity":
+            a, b = list(a), list(b)
+        assert a == b, name
+    assert C.sizeof(cb.Config) == C.sizeof(lib_cfg)
+
+
 def test_null_arguments_rejected(cb):
     L = cb.lib()
     assert L.cfdg_solver_create(0, None, None, None, 0, None) == cb.ERR_INVALID

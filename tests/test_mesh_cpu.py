@@ -105,3 +105,40 @@ def test_connectivity_matches_reference(cb, refh):
         off, val = refh.connectivity(m, kind)
         off2, val2 = port.connectivity(m, kind)
         assert np.array_equal(off, off2) and np.array_equal(val, val2), kind
+
+
+def _geom(view, n, nf):
+    def arr(k, m):
+        return np.ctypeslib.as_array(getattr(view, k), shape=(m,)).copy()
+    cells = {k: arr(k, n) for k in ("cell_volume", "cell_centroid_x", "cell_centroid_y", "cell_centroid_z")}
+    faces = {k: arr(k, nf) for k in ("face_area", "face_centroid_x", "face_centroid_y", "face_centroid_z")}
+    return cells, faces, arr("face_patch", nf)
+
+
+@pytest.mark.parametrize("name", ["ramp", "plate", "bump", "sa_plate"])
+def test_reference_pipeline_mesh_equals_generator(cb, refh, name):
+    """The reference's own preprocessing (build_faces, migrate_local_mesh,
+    compute_mesh_geometry, reorder_local_mesh(RCM), validate) on the cases'
+    raw cells and nodes yields the mesh the product's generator builds: the
+    same cells, faces and patches with the same geometry, up to the cell
+    numbering.  The reference arm of the benchmark builds its meshes this way,
+    without the product library."""
+    case = cb.cases.ramp() if name == "ramp" else getattr(cb.cases, name)(scale=8)
+    rm = refh.RefMesh(case.spec)
+    hm = cb.HostMesh(case.spec)
+    assert (rm.n_cells, rm.n_faces, rm.n_inner) == (hm.n_cells, hm.n_faces, hm.n_inner)
+    assert rm.view.n_patches == hm.view.n_patches
+    rc, rf, rp = _geom(rm.view, rm.n_cells, rm.n_faces)
+    hc, hf, hp = _geom(hm.view, hm.n_cells, hm.n_faces)
+    for k in rc:
+        assert np.allclose(np.sort(rc[k]), np.sort(hc[k]), rtol=1e-13, atol=1e-13 * np.abs(hc[k]).max()), k
+    for k in rf:
+        assert np.allclose(np.sort(rf[k]), np.sort(hf[k]), rtol=1e-13, atol=1e-13 * np.abs(hf[k]).max()), k
+    assert np.array_equal(np.bincount(rp[rp >= 0]), np.bincount(hp[hp >= 0]))
+    # the same cells: centroid sets agree as a whole (lexicographic sort of
+    # the centroids rounded well above the two codes' round-off)
+    def order(c):
+        key = [np.round(c[k] / 1e-9) for k in ("cell_centroid_z", "cell_centroid_y", "cell_centroid_x")]
+        return np.lexsort(key)
+    rk, hk = order(rc), order(hc)
+    assert np.allclose(rc["cell_volume"][rk], hc["cell_volume"][hk], rtol=1e-12)

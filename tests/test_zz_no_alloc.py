@@ -41,3 +41,24 @@ def test_noalloc_norms_match_allocating_entry_point(cb):
     assert rc == cb.ERR_INVALID and b"4194304" in L.cfdg_last_error()
     rc = L.cfdg_residual_norms_noalloc(C.c_void_p(dev.data_ptr()), n, 7, None, out.ctypes.data_as(C.POINTER(C.c_double)))
     assert rc == cb.ERR_INVALID
+
+
+def test_noalloc_norms_at_the_size_limit_on_a_side_stream(cb):
+    # the largest accepted size (every one of the 16,384 x 6 partial slots in
+    # use, next to the result slots) on a non-default stream, against numpy
+    import torch
+
+    L = cb.lib()
+    n, nv = 4194304, 6
+    rng = np.random.default_rng(11)
+    res = rng.standard_normal((nv, n)) * np.array([1.0, 1e3, 1e-3, 5.0, 1e5, 1e-6])[:, None]
+    expect = np.sqrt((res ** 2).sum(axis=1) / n)
+    dev = torch.from_numpy(res.ravel()).to("cuda:0")
+    side = torch.cuda.Stream(device="cuda:0")
+    torch.cuda.synchronize()
+    out = np.zeros(6)
+    for _ in range(2):  # two calls in a row share the scratch
+        rc = L.cfdg_residual_norms_noalloc(C.c_void_p(dev.data_ptr()), n, nv, C.c_void_p(side.cuda_stream),
+                                           out.ctypes.data_as(C.POINTER(C.c_double)))
+        assert rc == cb.OK, L.cfdg_last_error()
+        assert np.allclose(out, expect, rtol=1e-12, atol=0.0)
