@@ -180,6 +180,13 @@ _SIGS = {
     "cfdg_solver_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "cfdg_solver_profile_read": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_int64), _dp]),
     "cfdg_solver_sgs_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "cfdg_recon_create": (C.c_int, [C.c_int, C.POINTER(MeshHost), C.c_int32, C.c_int32, C.c_double,
+                                    C.POINTER(C.c_void_p)]),
+    "cfdg_recon_destroy": (C.c_int, [C.c_void_p]),
+    "cfdg_gradient": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                C.POINTER(C.c_void_p), C.c_int32, C.c_void_p]),
+    "cfdg_limiter": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                               C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32, C.c_void_p]),
     "cfdg_bsr_create": (C.c_int, [C.c_int, C.c_int32, C.c_int32, _ip, _ip, C.c_int32, C.POINTER(C.c_void_p)]),
     "cfdg_bsr_destroy": (C.c_int, [C.c_void_p]),
     "cfdg_bsr_set_values": (C.c_int, [C.c_void_p, _dp]),
@@ -580,6 +587,45 @@ class Dataset:
         t = np.zeros((rows, MLP_OUT), dtype=np.float32)
         check(lib().cfdg_dataset_read_host(self._h, _u16(f), _f32(t), rows))
         return f, t
+
+
+def _ptr_array(ptrs):
+    arr = (C.c_void_p * len(ptrs))(*[C.c_void_p(int(p)) for p in ptrs])
+    return arr
+
+
+class Recon:
+    """cfdg_recon: GradientOperator::apply_set and Muscl::compute_limiters
+    on caller-owned device arrays (integer device addresses, one per
+    variable, n_cells doubles each)."""
+
+    def __init__(self, mesh: HostMesh, gradient: int = GRAD_LSQ_NODE, limiter: int = LIM_VENKATAKRISHNAN,
+                 venkat_k: float = 0.5, device: int = 0):
+        h = C.c_void_p()
+        check(lib().cfdg_recon_create(device, C.byref(mesh.view), gradient, limiter, venkat_k, C.byref(h)))
+        self._h = h
+        self.mesh = mesh
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cfdg_recon_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def gradient(self, q, gx, gy, gz, stream: int = 0):
+        n = len(q)
+        check(lib().cfdg_gradient(self._h, _ptr_array(q), _ptr_array(gx), _ptr_array(gy), _ptr_array(gz), n,
+                                  C.c_void_p(stream or None)))
+
+    def limiter(self, q, gx, gy, gz, phi, stream: int = 0):
+        n = len(q)
+        check(lib().cfdg_limiter(self._h, _ptr_array(q), _ptr_array(gx), _ptr_array(gy), _ptr_array(gz),
+                                 _ptr_array(phi), n, C.c_void_p(stream or None)))
 
 
 class Bsr:

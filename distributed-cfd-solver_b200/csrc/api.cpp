@@ -10,6 +10,7 @@
 
 #include "cfdg.h"
 #include "host_mesh.hpp"
+#include "recon.hpp"
 #include "solver.hpp"
 
 struct cfdg_solver {
@@ -32,6 +33,9 @@ struct cfdg_mlp {
 struct cfdg_dataset {
     cfdg::Dataset* impl;
     int device;
+};
+struct cfdg_recon {
+    cfdg::ReconOperator* impl;
 };
 
 namespace cfdg {
@@ -640,6 +644,45 @@ int cfdg_solver_attach_guess(cfdg_solver* s, cfdg_mlp* m) {
 int cfdg_solver_attach_dataset(cfdg_solver* s, cfdg_dataset* d, int32_t stride) {
     if (d && !d->impl) return CFDG_ERR_INVALID;
     CFDG_SOLVER_CALL(s, s->impl->attach_dataset(d ? d->impl : nullptr, stride));
+}
+
+// ------------------------------------------------- gradient / limiter operators
+int cfdg_recon_create(int device, const cfdg_mesh_host* mesh_h, int32_t gradient, int32_t limiter, double venkat_k,
+                      cfdg_recon** out) {
+    if (!mesh_h || !out) return CFDG_ERR_INVALID;
+    *out = nullptr;
+    const int dv = require_device(device);
+    if (dv != CFDG_OK) return dv;
+    return guarded([&] {
+        auto* r = new cfdg_recon{nullptr};
+        try {
+            r->impl = new cfdg::ReconOperator(device, *mesh_h, gradient, limiter, venkat_k);
+        } catch (...) {
+            delete r;
+            throw;
+        }
+        *out = r;
+    });
+}
+
+int cfdg_recon_destroy(cfdg_recon* r) {
+    if (!r) return CFDG_OK;
+    if (r->impl) cudaSetDevice(r->impl->device());
+    delete r->impl;
+    delete r;
+    return CFDG_OK;
+}
+
+int cfdg_gradient(cfdg_recon* r, const double* const* q_d, double* const* gx_d, double* const* gy_d,
+                  double* const* gz_d, int32_t nvars, void* stream) {
+    if (!r || !r->impl) return CFDG_ERR_INVALID;
+    return guarded([&] { r->impl->gradient(q_d, gx_d, gy_d, gz_d, nvars, static_cast<cudaStream_t>(stream)); });
+}
+
+int cfdg_limiter(cfdg_recon* r, const double* const* q_d, const double* const* gx_d, const double* const* gy_d,
+                 const double* const* gz_d, double* const* phi_d, int32_t nvars, void* stream) {
+    if (!r || !r->impl) return CFDG_ERR_INVALID;
+    return guarded([&] { r->impl->limiter(q_d, gx_d, gy_d, gz_d, phi_d, nvars, static_cast<cudaStream_t>(stream)); });
 }
 
 }  // extern "C"

@@ -21,15 +21,6 @@ void cuda_check(cudaError_t e, const char* what) {
 
 namespace {
 
-template <typename T>
-void upload_or_throw(DevArray<T>& a, const std::vector<T>& h, cudaStream_t s, const char* what) {
-    if (!a.upload(h, s)) throw Failure{CFDG_ERR_NOMEM, std::string("device allocation failed: ") + what};
-}
-template <typename T>
-void alloc_or_throw(DevArray<T>& a, std::size_t n, const char* what) {
-    if (!a.alloc(n)) throw Failure{CFDG_ERR_NOMEM, std::string("device allocation failed: ") + what};
-}
-
 // invert3x3 of the least-squares setup (gradient_operator.cpp:20-47).
 bool invert3x3(const double A[9], double inv[9]) {
     const double eps = 1.0e-14;
@@ -101,6 +92,52 @@ void lsq_coefficients(const HostMesh& m, const Csr& st, std::vector<double>& wx,
         }
     }
 }
+
+}  // namespace
+
+// LSQ coefficients of the stencil `st` laid out in warp slices (see
+// DevMesh::g_soff).
+LsqSlices build_lsq_slices(const HostMesh& hm, const Csr& st) {
+    std::vector<double> wx, wy, wz;
+    lsq_coefficients(hm, st, wx, wy, wz);
+    LsqSlices out;
+    const int32_t n = hm.n_cells;
+    const int32_t ns = (n + 31) / 32;
+    out.soff.assign(static_cast<std::size_t>(ns) + 1, 0);
+    for (int32_t sl = 0; sl < ns; ++sl) {
+        int32_t len = 0;
+        for (int32_t c = sl * 32; c < std::min(n, sl * 32 + 32); ++c) len = std::max(len, st.off[c + 1] - st.off[c]);
+        out.soff[sl + 1] = out.soff[sl] + int64_t(len) * 32;
+    }
+    const std::size_t slots = static_cast<std::size_t>(out.soff[ns]);
+    out.col.assign(slots, 0);
+    out.wx.assign(slots, 0.0);
+    out.wy.assign(slots, 0.0);
+    out.wz.assign(slots, 0.0);
+    for (int32_t sl = 0; sl < ns; ++sl) {
+        const int32_t len = static_cast<int32_t>((out.soff[sl + 1] - out.soff[sl]) / 32);
+        for (int l = 0; l < 32; ++l) {
+            const int32_t c = sl * 32 + l;
+            const int32_t cc = c < n ? c : n - 1;  // lanes past the last cell read a real cell
+            for (int32_t k = 0; k < len; ++k) {
+                const std::size_t q = static_cast<std::size_t>(out.soff[sl] + int64_t(k) * 32 + l);
+                const int32_t j = (c < n) ? st.off[c] + k : -1;
+                if (j >= 0 && j < st.off[c + 1]) {
+                    out.col[q] = st.val[j];
+                    out.wx[q] = wx[j];
+                    out.wy[q] = wy[j];
+                    out.wz[q] = wz[j];
+                } else {
+                    out.col[q] = cc;  // padding: own cell, zero weights
+                }
+            }
+        }
+    }
+    out.entries = static_cast<int64_t>(st.val.size());
+    return out;
+}
+
+namespace {
 
 struct Inflow {
     double p, u, v, w, T;
@@ -838,45 +875,13 @@ void Solver::setup_mesh(const cfdg_mesh_host& mesh) {
     upload_or_throw(c2c_, c2c.val, s, "c2c");
     if (need_grad_) {
         const Csr st = (cfg_.gradient == CFDG_GRAD_LSQ_FACE) ? c2c : build_cell_cells_node(hm);
-        std::vector<double> wx, wy, wz;
-        lsq_coefficients(hm, st, wx, wy, wz);
-        // warp slices (see DevMesh::g_soff)
-        const int32_t n = hm.n_cells;
-        const int32_t ns = (n + 31) / 32;
-        std::vector<int64_t> soff(static_cast<std::size_t>(ns) + 1, 0);
-        for (int32_t sl = 0; sl < ns; ++sl) {
-            int32_t len = 0;
-            for (int32_t c = sl * 32; c < std::min(n, sl * 32 + 32); ++c) len = std::max(len, st.off[c + 1] - st.off[c]);
-            soff[sl + 1] = soff[sl] + int64_t(len) * 32;
-        }
-        const std::size_t slots = static_cast<std::size_t>(soff[ns]);
-        std::vector<int32_t> scol(slots);
-        std::vector<double> swx(slots, 0.0), swy(slots, 0.0), swz(slots, 0.0);
-        for (int32_t sl = 0; sl < ns; ++sl) {
-            const int32_t len = static_cast<int32_t>((soff[sl + 1] - soff[sl]) / 32);
-            for (int l = 0; l < 32; ++l) {
-                const int32_t c = sl * 32 + l;
-                const int32_t cc = c < n ? c : n - 1;  // lanes past the last cell read a real cell
-                for (int32_t k = 0; k < len; ++k) {
-                    const std::size_t q = static_cast<std::size_t>(soff[sl] + int64_t(k) * 32 + l);
-                    const int32_t j = (c < n) ? st.off[c] + k : -1;
-                    if (j >= 0 && j < st.off[c + 1]) {
-                        scol[q] = st.val[j];
-                        swx[q] = wx[j];
-                        swy[q] = wy[j];
-                        swz[q] = wz[j];
-                    } else {
-                        scol[q] = cc;  // padding: own cell, zero weights
-                    }
-                }
-            }
-        }
-        g_entries_ = static_cast<int64_t>(st.val.size());
-        upload_or_throw(g_soff_, soff, s, "g_soff");
-        upload_or_throw(g_col_, scol, s, "g_col");
-        upload_or_throw(g_wx_, swx, s, "g_wx");
-        upload_or_throw(g_wy_, swy, s, "g_wy");
-        upload_or_throw(g_wz_, swz, s, "g_wz");
+        const LsqSlices sl = build_lsq_slices(hm, st);
+        g_entries_ = sl.entries;
+        upload_or_throw(g_soff_, sl.soff, s, "g_soff");
+        upload_or_throw(g_col_, sl.col, s, "g_col");
+        upload_or_throw(g_wx_, sl.wx, s, "g_wx");
+        upload_or_throw(g_wy_, sl.wy, s, "g_wy");
+        upload_or_throw(g_wz_, sl.wz, s, "g_wz");
         // the host vectors die at scope end: make the copies complete first
         cuda_check(cudaStreamSynchronize(s), "setup sync");
     }
@@ -948,10 +953,12 @@ void Solver::compute_alg_bytes(int64_t E, int64_t n_c2c, int64_t n_c2f) {
     const double visc = cfg_.viscous ? 1.0 : 0.0;
     ab_.prim = n * 5 * d * 2 + nb * (5 * d + i4 + 3 * d + 3 * d + i4 + 5 * d) + nb * 3 * d;
     ab_.grad = n * 5 * d + (n + 1) * i4 + double(E) * (i4 + 3 * d) + n * 15 * d;
+    // ghost gradients alone (the limiter frozen or not in use)
+    ab_.ghost_grad = nb * (15 * d + 5 * d + i4 + i4 + 3 * d + 3 * d + 3 * d);
     ab_.limiter = (muscl_ ? n * (5 + 15 + 3 + 1 + 5) * d + (n + 1) * i4 * 2 + double(n_c2c) * i4 +
                                 double(n_c2f) * i4 + F * 3 * d
                           : 0.0) +
-                  nb * (15 * d + 5 * d + i4 + i4 + 3 * d + 3 * d + 3 * d);
+                  ab_.ghost_grad;
     ab_.face_flux = F * (2 * i4 + 4 * d + 3 * d) + visc * F * 4 * d + (n + nb) * (5 + 15 + 5 + 3) * d + F * 6 * d;
     ab_.cell_gather = (n + 1) * i4 + double(n_c2f) * i4 + F * i4 + F * 6 * d + n * 6 * d;
     const double sa = (cfg_.precision == CFDG_PREC_MIXED) ? 4.0 : 8.0;
@@ -1319,7 +1326,8 @@ void Solver::stage(int st) {
             break;
         case CFDG_STAGE_LIMITER:
             if (need_grad_) {
-                ProfScope ps(&prof_, CFDG_KCAT_LIMITER, stream_, 1, ab_.limiter);
+                ProfScope ps(&prof_, CFDG_KCAT_LIMITER, stream_, 1,
+                             muscl_ && !limiter_frozen_ ? ab_.limiter : ab_.ghost_grad);
                 launch_limiter_ghostgrad(dm_, df_, gas_, muscl_ && !limiter_frozen_, cfg_.limiter, cfg_.venkat_k,
                                          stream_);
             }

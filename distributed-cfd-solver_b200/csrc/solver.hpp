@@ -21,6 +21,17 @@ namespace cfdg {
 
 void set_error(const std::string& msg);
 
+// Least-squares gradient coefficients in warp slices (DevMesh::g_soff):
+// slot offsets per slice, neighbour per slot, coefficients per slot, and
+// the stencil's entry count before padding.
+struct LsqSlices {
+    std::vector<int64_t> soff;
+    std::vector<int32_t> col;
+    std::vector<double> wx, wy, wz;
+    int64_t entries = 0;
+};
+LsqSlices build_lsq_slices(const HostMesh& hm, const Csr& st);
+
 // Owning device allocation.
 template <typename T>
 struct DevArray {
@@ -58,6 +69,15 @@ struct Failure {
     int status;
     std::string msg;
 };
+
+template <typename T>
+void upload_or_throw(DevArray<T>& a, const std::vector<T>& h, cudaStream_t s, const char* what) {
+    if (!a.upload(h, s)) throw Failure{CFDG_ERR_NOMEM, std::string("device allocation failed: ") + what};
+}
+template <typename T>
+void alloc_or_throw(DevArray<T>& a, std::size_t n, const char* what) {
+    if (!a.alloc(n)) throw Failure{CFDG_ERR_NOMEM, std::string("device allocation failed: ") + what};
+}
 void cuda_check(cudaError_t e, const char* what);
 
 // Optional per-launch timing with CUDA events recorded on the launching
@@ -301,7 +321,7 @@ private:
     Profiler prof_;
     // algorithmic (unique-touch) bytes per launch of each residual-side kernel
     struct {
-        double prim, grad, limiter, face_flux, cell_gather, jac, dt_rhs, state_update, norms;
+        double prim, grad, limiter, ghost_grad, face_flux, cell_gather, jac, dt_rhs, state_update, norms;
         double sa_pre, sa_grad, sa_face;
     } ab_{};
     void compute_alg_bytes(int64_t n_grad_edges, int64_t n_c2c, int64_t n_c2f);

@@ -341,6 +341,34 @@ CFDG_API int cfdg_solver_profile_read(cfdg_solver* s, double* ms_h, int64_t* lau
 /* Number of SGS colours / forward levels of the active ordering. */
 CFDG_API int cfdg_solver_sgs_info(const cfdg_solver* s, int32_t* n_groups_fwd_h, int32_t* n_groups_bwd_h);
 
+/* ------------------------------------------ gradient and limiter operators
+ * The reconstruction steps of the residual on fields the caller owns, for
+ * callers that keep their own state (the GradientOperator and
+ * ReconstructionPolicy seams of the reference).  Fields are device arrays
+ * of n_cells doubles, one per variable; q_d, gx_d, gy_d, gz_d and phi_d are
+ * HOST arrays of nvars such device pointers.  At one partition the cells
+ * are the owned cells and no BC ghost enters either stencil (as in the
+ * reference).  Launches are queued on `stream` (NULL: legacy default
+ * stream) and the calls return without synchronising. */
+typedef struct cfdg_recon cfdg_recon;
+/* GradientOperator::setup (include/cfd/numerics/gradient/gradient_operator.hpp:16-44,
+ * LSQ set-up src/numerics/gradient/gradient_operator.cpp:414-499,622-707)
+ * plus the limiter's face connectivity: gradient CFDG_GRAD_LSQ_FACE or
+ * CFDG_GRAD_LSQ_NODE, limiter CFDG_LIM_*, venkat_k the Venkatakrishnan K. */
+CFDG_API int cfdg_recon_create(int device, const cfdg_mesh_host* mesh_h, int32_t gradient, int32_t limiter,
+                               double venkat_k, cfdg_recon** out);
+CFDG_API int cfdg_recon_destroy(cfdg_recon* r);
+/* GradientOperator::apply_set (gradient_operator.hpp:38-43): the gradient of
+ * each q_d[v] on the cells into gx_d[v], gy_d[v], gz_d[v]. */
+CFDG_API int cfdg_gradient(cfdg_recon* r, const double* const* q_d, double* const* gx_d, double* const* gy_d,
+                           double* const* gz_d, int32_t nvars, void* stream);
+/* Muscl<Limiter>::compute_limiters (include/cfd/numerics/reconstruction/muscl.hpp:25-105):
+ * phi_d[v] from q_d[v] and its gradient (face-neighbour extrema, minimum of
+ * the limiter function over the cell's faces). */
+CFDG_API int cfdg_limiter(cfdg_recon* r, const double* const* q_d, const double* const* gx_d,
+                          const double* const* gy_d, const double* const* gz_d, double* const* phi_d, int32_t nvars,
+                          void* stream);
+
 /* ------------------------------------------------ block-sparse linear algebra */
 /* BsrMatrix + assemble (src/linalg/bsr_matrix.cpp:22-40): structure from
  * host CSR (sorted columns, diagonal present), values set later. */

@@ -112,6 +112,7 @@ def test_rejected_guess_is_the_zero_guess(cb):
     """A network whose guess is worse than zero is rejected every step and
     the solve is bitwise the zero-guess solve."""
     case = cb.cases.ramp(scale=2)
+    case.cfg.pre_freeze = cb.PREFREEZE_CONFIGURED  # the guess from the first step on
     mesh = cb.HostMesh(case.spec)
     p = _params(13, 5)
     p[M.OFF_B3:M.OFF_B3 + 5] = 1e3  # a huge constant update
@@ -128,6 +129,7 @@ def test_solver_collects_trains_and_uses_the_guess(cb):
     """Samples written by the solver train a network whose guess the solver
     accepts; the Krylov iterations of the same steps drop."""
     case = cb.cases.ramp()
+    case.cfg.pre_freeze = cb.PREFREEZE_CONFIGURED
     mesh = cb.HostMesh(case.spec)
     steps = 120
     ds = cb.Dataset(5, mesh.n_cells * steps)
@@ -168,3 +170,34 @@ def test_trained_guess_cuts_krylov_work_on_an_unseen_case(cb):
             assert runs[learned].converged
     assert runs[True].krylov_iterations_total < 0.95 * runs[False].krylov_iterations_total, (
         runs[False].krylov_iterations_total, runs[True].krylov_iterations_total)
+
+
+def test_pre_freeze_phase_is_the_fp64_path(cb):
+    """CFDG_PREFREEZE_FP64: until the limiter freezes, a mixed-precision
+    solver with a learned guess attached takes bitwise the plain FP64
+    solver's iterates (FP64 matrix, zero guess); from the freeze on it uses
+    the FP32 matrix and the guess."""
+    case = cb.cases.ramp(scale=2)
+    mesh = cb.HostMesh(case.spec)
+    net = cb.Mlp(5, seed=1)
+    net.set_params(_params(13, 5))
+    F = case.cfg.limiter_freeze
+    states = {}
+    for name, prec, learned in (("fp64", 0, False), ("mixed", 1, True)):
+        case.cfg.precision = prec
+        with cb.Solver(mesh, case.cfg, case.bcs) as s:
+            s.init_fields()
+            if learned:
+                s.attach_guess(net)
+            guess = []
+            for it in range(1, F + 3):
+                if it == F:
+                    s.freeze_limiter(True)
+                guess.append(s.newton_step(cb.cases.cfl_at(case.cfg, it)).guess_used)
+                if it == F - 1:
+                    states[name] = s.get(cb.FIELD_U)
+            states[name + "_after"] = s.get(cb.FIELD_U)
+            if learned:
+                assert all(g == 0 for g in guess[:F - 1]) and all(g in (1, 2) for g in guess[F - 1:]), guess
+    assert np.array_equal(states["fp64"], states["mixed"])
+    assert not np.array_equal(states["fp64_after"], states["mixed_after"])
