@@ -60,7 +60,9 @@ namespace sc = cfd::solver::compressible;
 
 #define REFH_API extern "C" __attribute__((visibility("default")))
 
-namespace {
+// MeshPart / SolverConfig / BoundaryConfig from the C structures (external
+// linkage: the adapter harness refbind_harness.cpp reuses them).
+namespace refh {
 
 mesh::MeshPart build_meshpart(const cfdg_mesh_host& v, bool with_geometry) {
     mesh::MeshPart mp;
@@ -186,6 +188,13 @@ sc::SolverConfig build_cfg(const cfdg_config& c) {
     s.residual_interval = 1;
     return s;
 }
+
+}  // namespace refh
+
+namespace {
+using refh::build_bcfg;
+using refh::build_cfg;
+using refh::build_meshpart;
 
 // Limiter freeze through the reference's reconstruction-policy seam
 // (ReconstructionPolicy, include/cfd/numerics/reconstruction/concepts.hpp):
