@@ -47,6 +47,7 @@ KRYLOV_CONVERGED, KRYLOV_DIVERGED, KRYLOV_MAX_ITERATIONS = 0, 1, 2
 JAC_REFERENCE, JAC_THIN_LAYER = 0, 1
 KRYLOV_DEVICE_LOOP, KRYLOV_HOST_LOOP = 0, 1
 PREFREEZE_CONFIGURED, PREFREEZE_FP64 = 0, 1
+TIME_STEADY, TIME_UNSTEADY = 0, 1
 STAGE_PRIMITIVES, STAGE_GRADIENT, STAGE_LIMITER, STAGE_FLUXES = range(4)
 KCAT_NAMES = ("primitives", "gradient", "limiter", "face_flux", "cell_gather", "jacobian", "lu", "spmv", "sgs",
               "krylov", "update", "turbulence", "guess")
@@ -90,7 +91,15 @@ class Config(C.Structure):
                 ("prandtl_turb", C.c_double), ("init_rho", C.c_double), ("init_p", C.c_double),
                 ("init_velocity", C.c_double * 3), ("venkat_k", C.c_double), ("cfl", C.c_double),
                 ("cfl_max", C.c_double), ("residual_tolerance", C.c_double), ("lin_rel_tol", C.c_double),
-                ("lin_abs_tol", C.c_double), ("nu_inf_ratio", C.c_double), ("max_iterations", C.c_int64)]
+                ("lin_abs_tol", C.c_double), ("nu_inf_ratio", C.c_double), ("max_iterations", C.c_int64),
+                ("dt_physical", C.c_double), ("max_time_steps", C.c_int64), ("time_mode", C.c_int32),
+                ("bdf_order", C.c_int32)]
+
+
+class UnsteadyResult(C.Structure):
+    _fields_ = [("time_steps", C.c_int64), ("subiterations_total", C.c_int64), ("krylov_iterations_total", C.c_int64),
+                ("steps_converged", C.c_int32), ("blowup", C.c_int32), ("t_physical", C.c_double),
+                ("seconds", C.c_double), ("l2_last", C.c_double * 6)]
 
 
 class KrylovResult(C.Structure):
@@ -154,6 +163,9 @@ _SIGS = {
     "cfdg_newton_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(StepResult)]),
     "cfdg_residual_norms": (C.c_int, [C.c_void_p, _dp]),
     "cfdg_run_steady": (C.c_int, [C.c_void_p, C.POINTER(RunResult)]),
+    "cfdg_run_unsteady": (C.c_int, [C.c_void_p, C.POINTER(UnsteadyResult)]),
+    "cfdg_solver_reset_time_levels": (C.c_int, [C.c_void_p]),
+    "cfdg_solver_write_vtu": (C.c_int, [C.c_void_p, C.POINTER(MeshHost), C.c_char_p, C.c_char_p]),
     "cfdg_solver_freeze_limiter": (C.c_int, [C.c_void_p, C.c_int32]),
     "cfdg_solver_set_limiter": (C.c_int, [C.c_void_p, _dp, C.c_int64]),
     "cfdg_tc_selftest": (C.c_int, [C.c_int, C.c_int32, C.c_int32, _u16p, _u16p, _fp]),
@@ -240,7 +252,8 @@ CONFIG_DEFAULTS = dict(
     krylov_loop=KRYLOV_DEVICE_LOOP, pre_freeze=PREFREEZE_CONFIGURED, reserved_=0,
     gamma=1.4, gas_constant=287.052874, prandtl=0.71, prandtl_turb=0.9, init_rho=1.225, init_p=101325.0,
     init_velocity=(0.0, 0.0, 0.0), venkat_k=0.5, cfl=0.4, cfl_max=0.4, residual_tolerance=1.0e-10,
-    lin_rel_tol=1.0e-1, lin_abs_tol=1.0e-15, nu_inf_ratio=3.0, max_iterations=10000)
+    lin_rel_tol=1.0e-1, lin_abs_tol=1.0e-15, nu_inf_ratio=3.0, max_iterations=10000,
+    dt_physical=1.0e-6, max_time_steps=1, time_mode=TIME_STEADY, bdf_order=2)
 
 
 def default_config(**overrides) -> Config:
@@ -441,6 +454,18 @@ class Solver:
         r = RunResult()
         check(lib().cfdg_run_steady(self._h, C.byref(r)))
         return r
+
+    def run_unsteady(self) -> UnsteadyResult:
+        r = UnsteadyResult()
+        check(lib().cfdg_run_unsteady(self._h, C.byref(r)))
+        return r
+
+    def reset_time_levels(self):
+        check(lib().cfdg_solver_reset_time_levels(self._h))
+
+    def write_vtu(self, outdir: str, stem: str):
+        """<outdir>/<stem>_00000.vtu + <stem>.pvtu of the current state."""
+        check(lib().cfdg_solver_write_vtu(self._h, C.byref(self.mesh.view), str(outdir).encode(), stem.encode()))
 
     def stream(self) -> int:
         return lib().cfdg_solver_stream(self._h) or 0

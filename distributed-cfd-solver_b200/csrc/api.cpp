@@ -147,6 +147,11 @@ void cfdg_config_default(cfdg_config* c) {
     c->lin_abs_tol = 1.0e-15;
     c->nu_inf_ratio = 3.0;
     c->max_iterations = 10000;
+    // SolverConfig [time] defaults (config.hpp:117-125)
+    c->dt_physical = 1.0e-6;
+    c->max_time_steps = 1;
+    c->time_mode = CFDG_TIME_STEADY;
+    c->bdf_order = 2;
 }
 
 // ------------------------------------------------------------------ meshes
@@ -282,6 +287,20 @@ int cfdg_run_steady(cfdg_solver* s, cfdg_run_result* out_h) {
         if (out_h) *out_h = r;
     });
 }
+
+int cfdg_run_unsteady(cfdg_solver* s, cfdg_unsteady_result* out_h) {
+    CFDG_SOLVER_CALL(s, {
+        const cfdg_unsteady_result r = s->impl->run_unsteady();
+        if (out_h) *out_h = r;
+    });
+}
+
+int cfdg_solver_write_vtu(cfdg_solver* s, const cfdg_mesh_host* mesh_h, const char* outdir, const char* stem) {
+    if (!mesh_h || !outdir || !stem) return CFDG_ERR_INVALID;
+    CFDG_SOLVER_CALL(s, s->impl->write_vtu(*mesh_h, outdir, stem));
+}
+
+int cfdg_solver_reset_time_levels(cfdg_solver* s) { CFDG_SOLVER_CALL(s, s->impl->reset_time_levels()); }
 
 void* cfdg_solver_stream(cfdg_solver* s) { return (s && s->impl) ? static_cast<void*>(s->impl->stream()) : nullptr; }
 

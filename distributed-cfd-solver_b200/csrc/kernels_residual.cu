@@ -272,14 +272,15 @@ __global__ void k_norm_finalize(int nblocks, int nv, const double* __restrict__ 
 // compute_dt (solver.hpp:263-277) fused with set_rhs_and_zero_du
 // (implicit_euler.hpp:81-92): alpha = max(lam,floor)/CFL, b = -R (AoS), du = 0.
 template <int NV>
-__global__ void k_dt_rhs(DevMesh m, DevFields f, double cfl, double* __restrict__ b, double* __restrict__ du) {
+__global__ void k_dt_rhs(DevMesh m, DevFields f, double cfl, double diag, double* __restrict__ b,
+                         double* __restrict__ du) {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.n) return;
     const int64_t n = m.n;
     const double inv_cfl = 1.0 / cfl;
     const double l = fmax(f.lam[c], kLamFloor);
     f.dt[c] = cfl * m.vol[c] / l;
-    f.alpha[c] = (l * inv_cfl) + (m.vol[c] * 0.0);
+    f.alpha[c] = (l * inv_cfl) + (m.vol[c] * diag);  // diag: BDF coefficient / dt (0 when steady)
     if (b) {
         const int64_t r = row_index(m, c);
 #pragma unroll
@@ -366,10 +367,30 @@ void launch_norms(int32_t n, int nv, const double* res, double* partials, double
     k_norm_finalize<<<1, 32 * 6, 0, s>>>(static_cast<int>(gr), nv, partials, 1.0 / double(n > 0 ? n : 1), l2);
 }
 
-void launch_dt_rhs(const DevMesh& m, const DevFields& f, int nv, double cfl, double* b, double* du, cudaStream_t s) {
+void launch_dt_rhs(const DevMesh& m, const DevFields& f, int nv, double cfl, double diag, double* b, double* du,
+                   cudaStream_t s) {
     const unsigned gr = grid_for(m.n, 256);
-    if (nv == 6) k_dt_rhs<6><<<gr, 256, 0, s>>>(m, f, cfl, b, du);
-    else k_dt_rhs<5><<<gr, 256, 0, s>>>(m, f, cfl, b, du);
+    if (nv == 6) k_dt_rhs<6><<<gr, 256, 0, s>>>(m, f, cfl, diag, b, du);
+    else k_dt_rhs<5><<<gr, 256, 0, s>>>(m, f, cfl, diag, b, du);
+}
+
+// Dual-time pseudo-source (Solver::add_unsteady_source_term,
+// solver.hpp:546-580): res += V (c0 U + c1 U^n + c2 U^{n-1}); BDF1 has c2 = 0
+// and reads no U^{n-1}.
+__global__ void k_unsteady_source(int32_t n, int nv, const double* __restrict__ vol, const double* __restrict__ U,
+                                  const double* __restrict__ Un, const double* __restrict__ Unm1, double c0,
+                                  double c1, double c2, double* __restrict__ res) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= int64_t(n) * nv) return;
+    const int32_t c = static_cast<int32_t>(t % n);
+    const double src = Unm1 ? (c0 * U[t] + c1 * Un[t] + c2 * Unm1[t]) : (c0 * U[t] + c1 * Un[t]);
+    res[t] += vol[c] * src;
+}
+
+void launch_unsteady_source(int32_t n, int nv, const double* vol, const double* U, const double* Un,
+                            const double* Unm1, double c0, double c1, double c2, double* res, cudaStream_t s) {
+    const int64_t len = int64_t(n) * nv;
+    if (len > 0) k_unsteady_source<<<grid_for(len, 256), 256, 0, s>>>(n, nv, vol, U, Un, Unm1, c0, c1, c2, res);
 }
 
 void launch_state_update(const DevMesh& m, double* U, const double* du, int nv, cudaStream_t s) {

@@ -187,4 +187,40 @@ void launch_sa_sweep(const DevMesh& m, const DevFields& f, const GasParams& g, c
     k_sa_cell<<<grid_for(m.n, 128), 128, 0, s>>>(m, f, sa, face, gnu, dsrc);
 }
 
+
+// Solution output fields of Solver::write_fields (solver.hpp:856-898) from
+// the conserved state: rho, u, v, w, pressure (eos::pressure), Mach
+// (|rho u| / (rho a), a = sqrt(gamma p / rho)), and with the turbulence model
+// nu_tilde and mu_t = rho nu_tilde f_v1 (SpalartAllmaras::append_output).
+__global__ void k_output_fields(int32_t n, int nv, const double* __restrict__ U, GasParams g, double cv1,
+                                double* __restrict__ out) {
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int64_t N = n;
+    const double r = U[c], ru = U[N + c], rv = U[2 * N + c], rw = U[3 * N + c], E = U[4 * N + c];
+    const double inv_rho = 1.0 / r;
+    const double q2 = (ru * ru + rv * rv + rw * rw) * (inv_rho * inv_rho);
+    const double e = (E * inv_rho) - 0.5 * q2;
+    const double p = (g.gamma - 1.0) * r * e;
+    const double a = sqrt(g.gamma * p / r);
+    out[c] = r;
+    out[N + c] = ru / r;
+    out[2 * N + c] = rv / r;
+    out[3 * N + c] = rw / r;
+    out[4 * N + c] = p;
+    out[5 * N + c] = sqrt(ru * ru + rv * rv + rw * rw) / (r * a);
+    if (nv == 6) {
+        const double nu = U[5 * N + c] / r;
+        const double T = p / (r * g.R);
+        const double chi = nu / (sutherland(T) / r), chi3 = chi * chi * chi;
+        out[6 * N + c] = nu;
+        out[7 * N + c] = r * nu * (chi3 / (chi3 + cv1 * cv1 * cv1));
+    }
+}
+
+void launch_output_fields(int32_t n, int nv, const double* U, const GasParams& g, double cv1, double* out,
+                          cudaStream_t s) {
+    if (n > 0) k_output_fields<<<grid_for(n, 256), 256, 0, s>>>(n, nv, U, g, cv1, out);
+}
+
 }  // namespace cfdg

@@ -771,6 +771,11 @@ Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, c
         throw Failure{CFDG_ERR_INVALID, "unknown Krylov loop driver"};
     if (cfg.pre_freeze != CFDG_PREFREEZE_CONFIGURED && cfg.pre_freeze != CFDG_PREFREEZE_FP64)
         throw Failure{CFDG_ERR_INVALID, "unknown pre-freeze mode"};
+    if (cfg.time_mode != CFDG_TIME_STEADY && cfg.time_mode != CFDG_TIME_UNSTEADY)
+        throw Failure{CFDG_ERR_INVALID, "unknown time mode"};
+    unsteady_ = cfg.time_mode == CFDG_TIME_UNSTEADY;
+    if (unsteady_ && (cfg.bdf_order < 1 || cfg.bdf_order > 2 || !(cfg.dt_physical > 0.0) || cfg.max_time_steps < 0))
+        throw Failure{CFDG_ERR_INVALID, "unsteady mode needs bdf_order 1 or 2, dt_physical > 0, max_time_steps >= 0"};
     muscl_ = cfg.reconstruction == CFDG_RECON_MUSCL;
     need_grad_ = muscl_ || cfg.viscous;
     if (cfg.gradient != CFDG_GRAD_LSQ_FACE && cfg.gradient != CFDG_GRAD_LSQ_NODE && need_grad_)
@@ -1224,7 +1229,18 @@ void Solver::init_fields() {
         launch_fill(U_.p + static_cast<std::size_t>(5) * dm_.n, dm_.n, rho * sap_.nu_inf, stream_);
     }
     cuda_check(cudaGetLastError(), "init launch");
+    if (unsteady_) reset_time_levels();  // Solver::init_fields fills U^n and U^{n-1} too (solver.hpp:525-537)
     cuda_check(cudaStreamSynchronize(stream_), "init sync");
+}
+
+void Solver::reset_time_levels() {
+    if (!unsteady_) throw Failure{CFDG_ERR_INVALID, "the solver is not in unsteady mode"};
+    const std::size_t bytes = U_.count * sizeof(double);
+    if (!Un_.p) alloc_or_throw(Un_, U_.count, "U^n");
+    if (!Unm1_.p) alloc_or_throw(Unm1_, U_.count, "U^n-1");
+    cuda_check(cudaMemcpyAsync(Un_.p, U_.p, bytes, cudaMemcpyDeviceToDevice, stream_), "D2D");
+    cuda_check(cudaMemcpyAsync(Unm1_.p, U_.p, bytes, cudaMemcpyDeviceToDevice, stream_), "D2D");
+    cuda_check(cudaStreamSynchronize(stream_), "time levels sync");
 }
 
 void Solver::set_limiter(const double* phi, int64_t count) {
@@ -1345,6 +1361,15 @@ void Solver::stage(int st) {
                 ProfScope ps(&prof_, CFDG_KCAT_TURBULENCE, stream_, 2, ab_.sa_face);
                 launch_sa_sweep(dm_, df_, gas_, sap_, rhonu_g_.p, gnu_, sa_face_.p, sa_jac_.p, sa_dsrc_.p, stream_);
             }
+            if (unsteady_) {  // step 9: the BDF pseudo-source (solver.hpp:242-246, 546-580)
+                const double idt = 1.0 / cfg_.dt_physical;
+                const bool bdf2 = bdf_cur_ == 2;
+                const double n = double(dm_.n) * nv_;
+                ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, n * 8.0 * (bdf2 ? 5.0 : 4.0) + dm_.n * 8.0);
+                launch_unsteady_source(dm_.n, nv_, vol_.p, U_.p, Un_.p, bdf2 ? Unm1_.p : nullptr,
+                                       (bdf2 ? 1.5 : 1.0) * idt, (bdf2 ? -2.0 : -1.0) * idt, bdf2 ? 0.5 * idt : 0.0,
+                                       res_.p, stream_);
+            }
             break;
         }
         default: throw Failure{CFDG_ERR_INVALID, "unknown stage"};
@@ -1363,7 +1388,9 @@ void Solver::compute_dt(double cfl) {
     if (!(cfl > 0.0)) throw Failure{CFDG_ERR_INVALID, "CFL must be positive"};
     cfl_now_ = cfl;
     ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, ab_.dt_rhs);
-    launch_dt_rhs(dm_, df_, nv_, cfl, b_.p, du_.p, stream_);
+    // implicit diagonal V/dt_pseudo, plus V c0/dt of the BDF term when unsteady (solver.hpp:267-277)
+    const double diag = unsteady_ ? (bdf_cur_ == 2 ? 1.5 : 1.0) / cfg_.dt_physical : 0.0;
+    launch_dt_rhs(dm_, df_, nv_, cfl, diag, b_.p, du_.p, stream_);
     cuda_check(cudaGetLastError(), "dt launch");
 }
 
@@ -1581,6 +1608,79 @@ cfdg_run_result Solver::run_steady() {
             break;
         }
     }
+    out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return out;
+}
+
+// Solver::run_dual_time (solver.hpp:662-736): per physical step BDF1 on the
+// first and BDF order afterwards, Newton sub-iterations until the monitor
+// (sub-iteration 1, every 5th and the last) drops below the tolerance, then
+// U^{n-1} <- U^n, U^n <- U (shift_physical_time_levels, solver.hpp:582-596).
+cfdg_unsteady_result Solver::run_unsteady() {
+    if (!unsteady_) throw Failure{CFDG_ERR_INVALID, "cfdg_run_unsteady: time_mode is not CFDG_TIME_UNSTEADY"};
+    if (!Un_.p) reset_time_levels();
+    cfdg_unsteady_result out{};
+    const auto t0 = std::chrono::steady_clock::now();
+    const bool robust = cfg_.convergence_monitor == 1;
+    const std::size_t bytes = U_.count * sizeof(double);
+    for (int64_t step = 1; step <= cfg_.max_time_steps; ++step) {
+        bdf_cur_ = (step == 1 || cfg_.bdf_order == 1) ? 1 : 2;
+        double ref_norm[6] = {0, 0, 0, 0, 0, 0};
+        bool have0 = false, converged = false;
+        for (int64_t sub = 1; sub <= cfg_.max_iterations; ++sub) {
+            cfdg_step_result st;
+            try {
+                st = newton_step(cfl_at(sub));
+            } catch (const Failure& f) {
+                if (f.status != CFDG_ERR_NONFINITE) throw;
+                out.blowup = 1;
+                break;
+            }
+            ++out.subiterations_total;
+            out.krylov_iterations_total += st.krylov_iterations;
+            for (int v = 0; v < nv_; ++v) out.l2_last[v] = st.l2[v];
+            const bool diagnose = sub == 1 || sub % 5 == 0 || sub == cfg_.max_iterations;
+            if (!diagnose) continue;
+            bool finite = true;
+            for (int v = 0; v < nv_; ++v) finite = finite && std::isfinite(st.l2[v]);
+            if (!finite) {
+                out.blowup = 1;
+                break;
+            }
+            double mon[6];
+            int nm = 0;
+            if (robust) {
+                mon[nm++] = st.l2[0];
+                mon[nm++] = std::sqrt(st.l2[1] * st.l2[1] + st.l2[2] * st.l2[2] + st.l2[3] * st.l2[3]);
+                mon[nm++] = st.l2[4];
+                if (nv_ == 6) mon[nm++] = st.l2[5];
+            } else {
+                for (int v = 0; v < nv_; ++v) mon[nm++] = st.l2[v];
+            }
+            if (!have0) {
+                for (int k = 0; k < nm; ++k) ref_norm[k] = mon[k];
+                have0 = true;
+                continue;
+            }
+            double rel = 0.0;
+            for (int k = 0; k < nm; ++k) {
+                if (robust) ref_norm[k] = std::max(ref_norm[k], mon[k]);
+                rel = std::max(rel, mon[k] / std::max(ref_norm[k], 1.0e-300));
+            }
+            if (rel <= cfg_.residual_tolerance) {
+                converged = true;
+                break;
+            }
+        }
+        if (out.blowup) break;
+        out.time_steps = step;
+        out.t_physical = double(step) * cfg_.dt_physical;
+        if (converged) ++out.steps_converged;
+        // U^{n-1} <- U^n, U^n <- U
+        std::swap(Un_.p, Unm1_.p);
+        cuda_check(cudaMemcpyAsync(Un_.p, U_.p, bytes, cudaMemcpyDeviceToDevice, stream_), "D2D");
+    }
+    cuda_check(cudaStreamSynchronize(stream_), "unsteady sync");
     out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return out;
 }

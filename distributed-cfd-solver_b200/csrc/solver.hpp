@@ -252,6 +252,11 @@ public:
     cfdg_step_result newton_step(double cfl);
     void residual_norms(double* l2_host);
     cfdg_run_result run_steady();
+    cfdg_unsteady_result run_unsteady();
+    // Solver::write_fields: <outdir>/<stem>_00000.vtu + <stem>.pvtu of the
+    // current state on `mesh` (the mesh the solver was created with)
+    void write_vtu(const cfdg_mesh_host& mesh, const std::string& outdir, const std::string& stem);
+    void reset_time_levels();
     cudaStream_t stream() const { return stream_; }
     int64_t launches() const { return prof_.launches; }
     Profiler& profiler() { return prof_; }
@@ -284,6 +289,11 @@ private:
     bool need_grad_ = false;
     bool muscl_ = false;
     bool limiter_frozen_ = false;
+    // dual time stepping: physical time levels U^n, U^{n-1} and the BDF
+    // order of the current physical step
+    bool unsteady_ = false;
+    int bdf_cur_ = 1;
+    DevArray<double> Un_, Unm1_;
     Mlp* guess_ = nullptr;
     Dataset* dataset_ = nullptr;
     int32_t ds_stride_ = 1, ds_phase_ = 0;

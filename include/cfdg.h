@@ -159,6 +159,9 @@ enum { CFDG_JAC_REFERENCE = 0, CFDG_JAC_THIN_LAYER = 1 };
 /* BiCGSTAB iteration driver (cfdg_config.krylov_loop). */
 enum { CFDG_KRYLOV_DEVICE_LOOP = 0, CFDG_KRYLOV_HOST_LOOP = 1 };
 
+/* Time mode (cfdg_config.time_mode). */
+enum { CFDG_TIME_STEADY = 0, CFDG_TIME_UNSTEADY = 1 };
+
 /* Linear solves before the limiter freeze (cfdg_config.pre_freeze).
  * CONFIGURED: the configured matrix precision and initial guess throughout.
  * FP64: until the limiter is frozen the linear solves use the FP64 matrix
@@ -210,7 +213,15 @@ typedef struct cfdg_config {
     double residual_tolerance;
     double lin_rel_tol, lin_abs_tol;
     double nu_inf_ratio;      /* SA freestream nu_tilde / nu                   */
-    int64_t max_iterations;
+    int64_t max_iterations;   /* steady: iterations; unsteady: sub-iterations per time step */
+    /* Dual time stepping (TimeMode::Unsteady, include/cfd/solver/time_mode.hpp;
+     * SolverConfig [time] dt, max_time_steps, bdf_order): time_mode
+     * CFDG_TIME_STEADY or CFDG_TIME_UNSTEADY, BDF order 1 or 2 (the first
+     * physical step is BDF1), physical step dt_physical [s]. */
+    double dt_physical;
+    int64_t max_time_steps;
+    int32_t time_mode;
+    int32_t bdf_order;
 } cfdg_config;
 
 typedef struct cfdg_krylov_result {
@@ -236,6 +247,16 @@ typedef struct cfdg_run_result {
     int64_t krylov_iterations_total;
     double l2_first[6], l2_last[6];
 } cfdg_run_result;
+
+typedef struct cfdg_unsteady_result {
+    int64_t time_steps;               /* physical steps taken                    */
+    int64_t subiterations_total;      /* Newton sub-iterations over all steps    */
+    int64_t krylov_iterations_total;
+    int32_t steps_converged;          /* steps whose sub-iterations met the tolerance */
+    int32_t blowup;
+    double t_physical, seconds;
+    double l2_last[6];                /* norms of the last sub-iteration's residual */
+} cfdg_unsteady_result;
 
 typedef struct cfdg_solver cfdg_solver;   /* Solver<...> + BackwardEuler     */
 typedef struct cfdg_bsr cfdg_bsr;         /* BsrMatrix + SGS + BiCGSTAB      */
@@ -329,6 +350,26 @@ CFDG_API int cfdg_residual_norms_noalloc(const double* res_d, int32_t n_cells, i
                                          double* l2_h);
 /* Solver::run_steady (solver.hpp:597-660) with the CFL ramp. */
 CFDG_API int cfdg_run_steady(cfdg_solver* s, cfdg_run_result* out_h);
+/* Solver::run_dual_time (solver.hpp:662-736), cfg.time_mode ==
+ * CFDG_TIME_UNSTEADY: max_time_steps physical steps of dt_physical, each
+ * up to max_iterations Newton sub-iterations of the residual with the BDF
+ * pseudo-source (add_unsteady_source_term, solver.hpp:546-580) and the
+ * V c0 / dt diagonal (compute_dt, solver.hpp:267-277), stopped when the
+ * monitor (checked on sub-iteration 1, every 5th and the last) drops below
+ * residual_tolerance; then U^{n-1} <- U^n, U^n <- U
+ * (shift_physical_time_levels, solver.hpp:582-596). */
+CFDG_API int cfdg_run_unsteady(cfdg_solver* s, cfdg_unsteady_result* out_h);
+/* Solver::write_fields (solver.hpp:856-898) via io::vtk::write_solution_vtu
+ * (src/io/vtk/vtu.cpp:321-470) at one rank: writes <outdir>/<stem>_00000.vtu
+ * (ASCII VTK unstructured grid: the mesh's points and cells, CellData rank,
+ * rho, u, v, w, pressure, mach, and with Spalart-Allmaras nu_tilde and mu_t)
+ * and <outdir>/<stem>.pvtu.  The fields are formed on the device from the
+ * current state; mesh_h must be the mesh the solver was created with. */
+CFDG_API int cfdg_solver_write_vtu(cfdg_solver* s, const cfdg_mesh_host* mesh_h, const char* outdir,
+                                   const char* stem);
+/* U^n = U^{n-1} = U: the physical time levels of the current state
+ * (init_fields does this; call it after cfdg_solver_set_state). */
+CFDG_API int cfdg_solver_reset_time_levels(cfdg_solver* s);
 /* Stream all solver kernels are queued on (cudaStream_t as void*). */
 CFDG_API void* cfdg_solver_stream(cfdg_solver* s);
 /* Total solver kernel launches since creation (for launch accounting). */

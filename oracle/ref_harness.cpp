@@ -30,6 +30,7 @@
 #include "cfd/linalg/bicgstab.hpp"
 #include "cfd/linalg/bsr_matrix.hpp"
 #include "cfd/linalg/preconditioners.hpp"
+#include "cfd/io/vtk/vtu.hpp"
 #include "cfd/mesh/aux_connectivity.hpp"
 #include "cfd/mesh/aux_geometry.hpp"
 #include "cfd/mesh/faces.hpp"
@@ -186,6 +187,10 @@ sc::SolverConfig build_cfg(const cfdg_config& c) {
     s.output_dir = "/tmp/cfdg_ref_out";
     s.field_interval = 0;
     s.residual_interval = 1;
+    s.time_mode = c.time_mode == CFDG_TIME_UNSTEADY ? sc::TimeMode::Unsteady : sc::TimeMode::Steady;
+    s.dt = c.dt_physical;
+    s.max_time_steps = c.max_time_steps;
+    s.bdf_order = c.bdf_order;
     return s;
 }
 
@@ -222,6 +227,7 @@ struct RefBase {
     virtual void jacobian(double cfl, double* alpha, double* values) = 0;
     virtual int newton_step(double cfl, double* l2, int* kit, int* kstat, double* kinit, double* kfinal) = 0;
     virtual int64_t nnzb() const = 0;
+    virtual void write_vtu(const char* outdir, const char* stem) = 0;
     bool frozen = false;
 };
 
@@ -284,6 +290,29 @@ struct RefImpl final : RefBase {
     }
 
     int64_t nnzb() const override { return static_cast<int64_t>(mat->rowPtr()[n]); }
+
+    // Solver::write_fields (solver.hpp:856-898; private there): the same
+    // fields from the Solver's state through the reference's EOS helpers,
+    // written by the reference's io::vtk::write_solution_vtu.
+    void write_vtu(const char* outdir, const char* stem) override {
+        auto u = solver->u_slots();
+        std::vector<double> rho(n), vx(n), vy(n), vz(n), pr(n), mach(n);
+        for (std::size_t c = 0; c < n; ++c) {
+            const double U5[5] = {u[0][c], u[1][c], u[2][c], u[3][c], u[4][c]};
+            const double r = U5[0];
+            const double p = sc::eos::pressure(eos, U5);
+            const double a = eos.sound_speed_rhop(r, p);
+            rho[c] = r;
+            vx[c] = U5[1] / r;
+            vy[c] = U5[2] / r;
+            vz[c] = U5[3] / r;
+            pr[c] = p;
+            mach[c] = std::sqrt(U5[1] * U5[1] + U5[2] * U5[2] + U5[3] * U5[3]) / (r * a);
+        }
+        const io::vtk::SolutionField f[] = {{"rho", rho.data()}, {"u", vx.data()},        {"v", vy.data()},
+                                            {"w", vz.data()},     {"pressure", pr.data()}, {"mach", mach.data()}};
+        io::vtk::write_solution_vtu(mp, f, 6, outdir, stem, MPI_COMM_WORLD);
+    }
 
     void set_state(const double* Uin, int64_t ld) override {
         for (int v = 0; v < 5; ++v) {
@@ -468,6 +497,10 @@ REFH_API int refh_create(const cfdg_mesh_host* m, const cfdg_config* c, const cf
 
 REFH_API void refh_destroy(refh_solver* s) { delete s; }
 REFH_API int64_t refh_nnzb(refh_solver* s) { return s->impl->nnzb(); }
+REFH_API int refh_write_vtu(refh_solver* s, const char* outdir, const char* stem) {
+    s->impl->write_vtu(outdir, stem);
+    return 0;
+}
 REFH_API int refh_set_state(refh_solver* s, const double* U, int64_t ld) {
     s->impl->set_state(U, ld);
     return 0;
@@ -843,3 +876,41 @@ REFH_API int refh_mesh_view(const refh_mesh* m, cfdg_mesh_host* view) {
 }
 
 REFH_API void refh_mesh_free(refh_mesh* m) { delete m; }
+
+// ------------------------------------------------------------ dual time
+// Solver<..., BackwardEuler, UnsteadyMode<order>>::run: init_fields, then
+// run_dual_time (solver.hpp:662-736) over max_time_steps physical steps of
+// dt, each with up to max_iterations sub-iterations at the configured CFL.
+namespace {
+template <typename Phys, int Order>
+void run_unsteady_ref(const cfdg_mesh_host& m, const cfdg_config& c, const cfdg_bc_desc* bcs, int nbc,
+                      double* U_out) {
+    using Stack = sc::physics::PhysicsStack<Phys>;
+    using SolverT = sc::Solver<sc::eos::IdealGas, sc::fluxes::HllcFlux,
+                               numerics::recon::Muscl<numerics::limiter::Venkatakrishnan>, Stack,
+                               sc::time::BackwardEuler, solver::UnsteadyMode<Order>>;
+    const mesh::MeshPart mp = build_meshpart(m, true);
+    const sc::SolverConfig cfg = build_cfg(c);
+    const bc::BoundaryConfig bcfg = build_bcfg(bcs, nbc);
+    const sc::eos::IdealGas eos = cfg.flow.create_ideal_gas();
+    Stack phys;
+    if constexpr (Phys::kHasViscous) phys.base.prandtl = cfg.prandtl;
+    SolverT s(cfg, bcfg, eos, phys, mp, MPI_COMM_WORLD);
+    s.run();
+    const auto u = s.u_slots();
+    const std::size_t n = static_cast<std::size_t>(mp.n_own);
+    for (std::size_t v = 0; v < 5; ++v) std::copy(u[v], u[v] + n, U_out + v * n);
+}
+}  // namespace
+
+REFH_API int refh_run_unsteady(const cfdg_mesh_host* m, const cfdg_config* c, const cfdg_bc_desc* bcs, int nbc,
+                               double* U_out) {
+    if (c->bdf_order == 1) {
+        if (c->viscous) run_unsteady_ref<sc::physics::ViscousFlow, 1>(*m, *c, bcs, nbc, U_out);
+        else run_unsteady_ref<sc::physics::InviscidFlow, 1>(*m, *c, bcs, nbc, U_out);
+    } else {
+        if (c->viscous) run_unsteady_ref<sc::physics::ViscousFlow, 2>(*m, *c, bcs, nbc, U_out);
+        else run_unsteady_ref<sc::physics::InviscidFlow, 2>(*m, *c, bcs, nbc, U_out);
+    }
+    return 0;
+}

@@ -48,6 +48,8 @@ def _lib():
         L.refh_mesh_generate.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
         L.refh_mesh_view.argtypes = [C.c_void_p, C.c_void_p]
         L.refh_mesh_free.argtypes = [C.c_void_p]
+        L.refh_run_unsteady.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, _dp]
+        L.refh_write_vtu.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
         L.refh_bsr_spmv.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_double, C.c_double]
         L.refh_sgs_apply.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_int]
         L.refh_bicgstab.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, C.c_int, C.c_double, C.c_double, C.c_int, _dp,
@@ -201,6 +203,10 @@ class RefSolver:
         _lib().refh_jacobian(self._h, cfl, _d(alpha), _d(vals))
         return alpha, vals
 
+    def write_vtu(self, outdir, stem):
+        """The reference's write_solution_vtu of the Solver's current state."""
+        _lib().refh_write_vtu(self._h, str(outdir).encode(), stem.encode())
+
     def freeze_limiter(self, frozen=True):
         """Keep the Solver's limiter values of the last evaluation (the
         library's limiter freeze, applied through the reconstruction policy)."""
@@ -210,6 +216,17 @@ class RefSolver:
         l2 = np.zeros(5)
         _lib().refh_newton_step(self._h, cfl, _d(l2))
         return l2
+
+
+def run_unsteady(mesh, cfg, bcs):
+    """The reference Solver with BackwardEuler and UnsteadyMode<cfg.bdf_order>
+    run from init_fields: cfg.max_time_steps physical steps of
+    cfg.dt_physical, cfg.max_iterations sub-iterations each (fewer if the
+    reference monitor drops below cfg.residual_tolerance).  Returns U (5 x n)."""
+    U = np.zeros((5, mesh.n_cells))
+    arr = (type(bcs[0]) * len(bcs))(*bcs)
+    _lib().refh_run_unsteady(C.byref(mesh.view), C.byref(cfg), arr, len(bcs), _d(U))
+    return U
 
 
 def bsr_spmv(row_ptr, cols, vals, bs, x, y=None, alpha=1.0, beta=0.0):
