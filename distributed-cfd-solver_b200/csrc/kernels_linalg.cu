@@ -67,119 +67,30 @@ __device__ __forceinline__ void load_vec(const double* __restrict__ x, double (&
     }
 }
 
-// The same sum for a BS-lane group that owns one block row (lane ii of the
-// group, whose first lane is `base`, computes component ii): each lane loads
-// one entry of each neighbour block of x and the group exchanges them by
-// shuffles (mask `gmask`: the group's lanes, which run the same trip count).
-// Per block a lane issues the BS/2 paired loads of its matrix row and one
-// load of x; two blocks per step keep both blocks' loads in flight.
-#ifndef CFDG_ROWDOT_VARIANT
-#define CFDG_ROWDOT_VARIANT 2
-#endif
-constexpr int kRowDotVariant = CFDG_ROWDOT_VARIANT;
-
+// acc (+|-)= sum over blocks k in [k0, k1) of A_k[ii][:] . x_col(k) in
+// ascending block order, each block's partial sum formed first (the
+// arithmetic of the sequential sweep and product).  The block row and the
+// neighbour's x block load as 16-byte pairs for 6x6 blocks (measured on the
+// SA plate: SGS 0.73 -> 0.80 of the copy bandwidth); other block sizes keep
+// scalar loads, which measured faster for 5x5 (FP32 tet bump).
 template <typename MT, int BS, bool SUB>
-__device__ __forceinline__ double scalar_row_dot(const BsrView& A, const MT* __restrict__ vals,
-                                                 const double* x, int ii, int32_t k0, int32_t k1, double acc) {
+__device__ __forceinline__ double block_row_dot(const BsrView& A, const MT* __restrict__ vals, const double* x,
+                                                int ii, int32_t k0, int32_t k1, double acc) {
     for (int32_t k = k0; k < k1; ++k) {
-        const MT* a = vals + int64_t(k) * (BS * BS) + ii * BS;
-        const double* xb = x + int64_t(A.cols[k]) * BS;
         double t = 0.0;
+        if constexpr (BS == 6) {
+            double a[BS], xb[BS];
+            load_block_row<MT, BS>(vals + int64_t(k) * (BS * BS) + ii * BS, a);
+            load_vec<BS>(x + int64_t(__ldg(A.cols + k)) * BS, xb);
 #pragma unroll
-        for (int jj = 0; jj < BS; ++jj) t += ld(a + jj) * xb[jj];
+            for (int jj = 0; jj < BS; ++jj) t += a[jj] * xb[jj];
+        } else {
+            const MT* a = vals + int64_t(k) * (BS * BS) + ii * BS;
+            const double* xb = x + int64_t(A.cols[k]) * BS;
+#pragma unroll
+            for (int jj = 0; jj < BS; ++jj) t += ld(a + jj) * xb[jj];
+        }
         acc = SUB ? acc - t : acc + t;
-    }
-    return acc;
-}
-
-template <typename MT, int BS, bool SUB, int UNROLL = (kRowDotVariant >= 3 ? 2 : 1)>
-__device__ __forceinline__ double group_row_dot(const BsrView& A, const MT* __restrict__ vals,
-                                                const double* __restrict__ x, int ii, unsigned gmask, int base,
-                                                int32_t k0, int32_t k1, double acc) {
-    if constexpr (kRowDotVariant == 0) return scalar_row_dot<MT, BS, SUB>(A, vals, x, ii, k0, k1, acc);
-    if constexpr (kRowDotVariant == 1) {
-        int32_t k = k0;
-        for (; k < k1; ++k) {
-            double a0[BS], x0[BS];
-            load_block_row<MT, BS>(vals + int64_t(k) * (BS * BS) + ii * BS, a0);
-            load_vec<BS>(x + int64_t(__ldg(A.cols + k)) * BS, x0);
-            double t0 = 0.0;
-#pragma unroll
-            for (int jj = 0; jj < BS; ++jj) t0 += a0[jj] * x0[jj];
-            acc = SUB ? acc - t0 : acc + t0;
-        }
-        return acc;
-    }
-    int32_t k = k0;
-    for (; UNROLL == 2 && k + 1 < k1; k += 2) {
-        const int32_t c0 = __ldg(A.cols + k), c1 = __ldg(A.cols + k + 1);
-        double a0[BS], a1[BS];
-        load_block_row<MT, BS>(vals + int64_t(k) * (BS * BS) + ii * BS, a0);
-        load_block_row<MT, BS>(vals + int64_t(k + 1) * (BS * BS) + ii * BS, a1);
-        const double x0 = __ldg(x + int64_t(c0) * BS + ii), x1 = __ldg(x + int64_t(c1) * BS + ii);
-        double t0 = 0.0, t1 = 0.0;
-#pragma unroll
-        for (int jj = 0; jj < BS; ++jj) t0 += a0[jj] * __shfl_sync(gmask, x0, base + jj);
-#pragma unroll
-        for (int jj = 0; jj < BS; ++jj) t1 += a1[jj] * __shfl_sync(gmask, x1, base + jj);
-        if (SUB) {
-            acc -= t0;
-            acc -= t1;
-        } else {
-            acc += t0;
-            acc += t1;
-        }
-    }
-    for (; k < k1; ++k) {
-        double a0[BS];
-        load_block_row<MT, BS>(vals + int64_t(k) * (BS * BS) + ii * BS, a0);
-        const double x0 = __ldg(x + int64_t(__ldg(A.cols + k)) * BS + ii);
-        double t0 = 0.0;
-#pragma unroll
-        for (int jj = 0; jj < BS; ++jj) t0 += a0[jj] * __shfl_sync(gmask, x0, base + jj);
-        acc = SUB ? acc - t0 : acc + t0;
-    }
-    return acc;
-}
-
-// acc (+|-)= sum over blocks k in [k0, k1) of A_k[ii][:] . x_col(k), in
-// ascending block order with each block's partial sum formed first (the
-// arithmetic of the sequential kernels); two blocks per step so that both
-// blocks' loads are in flight together.
-template <typename MT, int BS, bool SUB, int UNROLL = (kRowDotVariant >= 3 ? 2 : 1)>
-__device__ __forceinline__ double block_row_dot(const BsrView& A, const MT* __restrict__ vals,
-                                                const double* __restrict__ x, int ii, int32_t k0, int32_t k1,
-                                                double acc) {
-    if constexpr (kRowDotVariant == 0) return scalar_row_dot<MT, BS, SUB>(A, vals, x, ii, k0, k1, acc);
-    int32_t k = k0;
-    for (; UNROLL == 2 && k + 1 < k1; k += 2) {
-        const int32_t c0 = __ldg(A.cols + k), c1 = __ldg(A.cols + k + 1);
-        double a0[BS], a1[BS], x0[BS], x1[BS];
-        load_block_row<MT, BS>(vals + int64_t(k) * (BS * BS) + ii * BS, a0);
-        load_block_row<MT, BS>(vals + int64_t(k + 1) * (BS * BS) + ii * BS, a1);
-        load_vec<BS>(x + int64_t(c0) * BS, x0);
-        load_vec<BS>(x + int64_t(c1) * BS, x1);
-        double t0 = 0.0, t1 = 0.0;
-#pragma unroll
-        for (int jj = 0; jj < BS; ++jj) t0 += a0[jj] * x0[jj];
-#pragma unroll
-        for (int jj = 0; jj < BS; ++jj) t1 += a1[jj] * x1[jj];
-        if (SUB) {
-            acc -= t0;
-            acc -= t1;
-        } else {
-            acc += t0;
-            acc += t1;
-        }
-    }
-    for (; k < k1; ++k) {
-        double a0[BS], x0[BS];
-        load_block_row<MT, BS>(vals + int64_t(k) * (BS * BS) + ii * BS, a0);
-        load_vec<BS>(x + int64_t(__ldg(A.cols + k)) * BS, x0);
-        double t0 = 0.0;
-#pragma unroll
-        for (int jj = 0; jj < BS; ++jj) t0 += a0[jj] * x0[jj];
-        acc = SUB ? acc - t0 : acc + t0;
     }
     return acc;
 }
@@ -219,7 +130,16 @@ __global__ void __launch_bounds__(kVecThreads) k_spmv(BsrView A, const MT* __res
     for (int64_t t = int64_t(row_begin) * BS + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < N; t += stride) {
         const int32_t row = static_cast<int32_t>(t / BS);
         const int ii = static_cast<int>(t % BS);
-        const double acc = block_row_dot<MT, BS, false>(A, vals, x, ii, A.row_ptr[row], A.row_ptr[row + 1], 0.0);
+        double acc = 0.0;
+        const int32_t k1 = A.row_ptr[row + 1];
+        for (int32_t k = A.row_ptr[row]; k < k1; ++k) {
+            const MT* a = vals + int64_t(k) * (BS * BS) + ii * BS;
+            const double* xb = x + int64_t(A.cols[k]) * BS;
+            double s = 0.0;
+#pragma unroll
+            for (int jj = 0; jj < BS; ++jj) s += ld(a + jj) * xb[jj];
+            acc += s;
+        }
         double yv;
         if (alpha == 1.0 && beta == 0.0) yv = acc;
         else if (beta == 1.0) yv = y[t] + alpha * acc;
@@ -431,14 +351,13 @@ __global__ void __launch_bounds__(256, (INV && BS <= 5) ? 8 : 6) k_sgs_rows(BsrV
         s = (MODE == 3) ? 0.0 : r[int64_t(i) * BS + ii];
         if (MODE != 1) {
             const int32_t d = A.diag[i];
-            const unsigned gmask = ((1u << BS) - 1u) << (grp * BS);
             if (MODE == 0) {  // lower then upper blocks, skipping the diagonal
-                s = group_row_dot<MT, BS, true>(A, vals, z, ii, gmask, grp * BS, A.row_ptr[i], d, s);
-                s = group_row_dot<MT, BS, true>(A, vals, z, ii, gmask, grp * BS, d + 1, A.row_ptr[i + 1], s);
+                s = block_row_dot<MT, BS, true>(A, vals, z, ii, A.row_ptr[i], d, s);
+                s = block_row_dot<MT, BS, true>(A, vals, z, ii, d + 1, A.row_ptr[i + 1], s);
             } else {
                 const int32_t k0 = (MODE == 3) ? d + 1 : A.row_ptr[i];
                 const int32_t k1 = (MODE == 2) ? d : A.row_ptr[i + 1];
-                s = group_row_dot<MT, BS, true>(A, vals, z, ii, gmask, grp * BS, k0, k1, s);
+                s = block_row_dot<MT, BS, true>(A, vals, z, ii, k0, k1, s);
             }
         }
     }
@@ -475,7 +394,7 @@ __global__ void __launch_bounds__(256, (INV && BS <= 5) ? 8 : 6) k_sgs_rows(BsrV
 // again.  Dot products of the result as k_spmv; the grid strides over the
 // rows so the partials number at most kVecGridCap.
 template <typename MT, int BS, int ND>
-__global__ void __launch_bounds__(256, BS <= 5 ? 8 : 6) k_sgs_last_spmv(BsrView A, const MT* __restrict__ vals,
+__global__ void __launch_bounds__(256, BS <= 5 ? 6 : 5) k_sgs_last_spmv(BsrView A, const MT* __restrict__ vals,
                                                                        const MT* __restrict__ dinv, int32_t n_rows,
                                                                        double* __restrict__ z, double* __restrict__ y,
                                                                        DotSpec ds, double* __restrict__ partials,
@@ -494,9 +413,7 @@ __global__ void __launch_bounds__(256, BS <= 5 ? 8 : 6) k_sgs_last_spmv(BsrView 
         const bool act = (grp < GPW) && (slot < n_rows);
         const int32_t i = act ? static_cast<int32_t>(slot) : 0;
         double s = 0.0;
-        if (act)
-            s = group_row_dot<MT, BS, true>(A, vals, z, ii, ((1u << BS) - 1u) << base, base, A.diag[i] + 1,
-                                            A.row_ptr[i + 1], 0.0);
+        if (act) s = block_row_dot<MT, BS, true>(A, vals, z, ii, A.diag[i] + 1, A.row_ptr[i + 1], 0.0);
         double b[BS];
 #pragma unroll
         for (int j = 0; j < BS; ++j) b[j] = __shfl_sync(0xffffffffu, s, base + j);
@@ -744,10 +661,14 @@ __global__ void k_krylov_cond(KrylovScalars* ks, cudaGraphConditionalHandle h) {
 // ------------------------------------------------------------- launchers
 int spmv_blocks(int32_t n, int32_t bs) { return static_cast<int>(vec_grid(int64_t(n) * bs)); }
 
+// One wave of the fused pass: its launch bounds let 6 (bs <= 5) or 5 (6x6)
+// 256-thread blocks share an SM, so the grid-stride loop runs on exactly the
+// resident blocks.
 int sgs_last_spmv_blocks(int32_t n_rows, int32_t bs) {
     const int64_t warps = (int64_t(n_rows) + (32 / bs) - 1) / (32 / bs);
     const int64_t g = (warps + 7) / 8;
-    return static_cast<int>(g < 1 ? 1 : (g < kVecGridCap ? g : kVecGridCap));
+    const int64_t cap = int64_t(148) * (bs <= 5 ? 6 : 5);
+    return static_cast<int>(g < 1 ? 1 : (g < cap ? g : cap));
 }
 
 template <typename MT>

@@ -417,12 +417,15 @@ void BsrSystem::build_ordering(int ordering) {
     // own z read of MODE 3), z write, and each distinct neighbour z block
     // once.  out[0]: full row, out[1]: no neighbours, out[2]: the split half
     // (columns below the diagonal forward, above it backward).
-    const double sa = (precision_ == CFDG_PREC_MIXED) ? 4.0 : 8.0;
-    const double b2 = double(bs_) * bs_;
+    // Kept as (bytes that do not depend on the matrix precision, matrix
+    // blocks read) so that a precision switch (set_precision) keeps them right.
     auto pass_bytes = [&](const std::vector<int32_t>& off, const std::vector<int32_t>& rows, bool lower,
-                          std::vector<double>* out) {
+                          std::vector<double>* out, std::vector<double>* blocks) {
         const int ng = static_cast<int>(off.size()) - 1;
-        for (int m = 0; m < 3; ++m) out[m].assign(ng, 0.0);
+        for (int m = 0; m < 3; ++m) {
+            out[m].assign(ng, 0.0);
+            blocks[m].assign(ng, 0.0);
+        }
         std::vector<int32_t> seen(n, -1), seen_half(n, -1);
         for (int g = 0; g < ng; ++g) {
             double offd = 0.0, nbr = 0.0, offd_h = 0.0, nbr_h = 0.0;
@@ -446,14 +449,17 @@ void BsrSystem::build_ordering(int ordering) {
                 }
             }
             // list, LU factors + pivots (level) or D^-1 (colour), r, z
-            const double own = R * (4.0 + b2 * sa + (ordering == CFDG_SGS_COLOR ? 0.0 : bs_) + 2.0 * 8.0 * bs_);
+            const double own = R * (4.0 + (ordering == CFDG_SGS_COLOR ? 0.0 : bs_) + 2.0 * 8.0 * bs_);
             out[1][g] = own;
-            out[0][g] = own + R * (8.0 + 4.0) + offd * (b2 * sa + 4.0) + nbr * 8.0 * bs_;
-            out[2][g] = own + R * (8.0 + 4.0) + offd_h * (b2 * sa + 4.0) + nbr_h * 8.0 * bs_;
+            blocks[1][g] = R;
+            out[0][g] = own + R * (8.0 + 4.0) + offd * 4.0 + nbr * 8.0 * bs_;
+            blocks[0][g] = R + offd;
+            out[2][g] = own + R * (8.0 + 4.0) + offd_h * 4.0 + nbr_h * 8.0 * bs_;
+            blocks[2][g] = R + offd_h;
         }
     };
-    pass_bytes(fwd_off_, fr, true, fwd_bytes_);
-    pass_bytes(bwd_off_, br, false, bwd_bytes_);
+    pass_bytes(fwd_off_, fr, true, fwd_bytes_, fwd_blocks_);
+    pass_bytes(bwd_off_, br, false, bwd_bytes_, bwd_blocks_);
     upload_or_throw(fwd_rows_, fr, stream_, "sgs rows");
     upload_or_throw(bwd_rows_, br, stream_, "sgs rows");
     ordering_ = ordering;
@@ -511,7 +517,7 @@ void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, doubl
                 if (sw > 0 && g == 0) continue;  // equal to the last backward colour pass
                 if (sw == 0) mode = (g == 0) ? 1 : (split ? 2 : 0);  // colour 0: all neighbours still zero
             }
-            ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, fwd_bytes_[mode][g]);
+            ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, fwd_bytes_[mode][g] + fwd_blocks_[mode][g] * block_bytes());
             const bool cg = fwd_first_[g] >= 0;
             launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, cg ? nullptr : fwd_rows_.p + fwd_off_[g], cg ? fwd_first_[g] : 0,
                                    fwd_off_[g + 1] - fwd_off_[g], r, z, mode, color, active, stream_);
@@ -519,7 +525,8 @@ void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, doubl
         for (int g = 0; g < nbk; ++g) {
             if (color && g == 0) continue;  // first backward colour == last forward colour
             if (skip_last && g == nbk - 1) continue;  // fused with the product (sgs_apply_spmv)
-            ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, bwd_bytes_[split ? 2 : 0][g]);
+            ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1,
+                         bwd_bytes_[split ? 2 : 0][g] + bwd_blocks_[split ? 2 : 0][g] * block_bytes());
             const bool cg = bwd_first_[g] >= 0;
             launch_sgs_rows_ex<MT>(A, vals, lu, piv_.p, cg ? nullptr : bwd_rows_.p + bwd_off_[g], cg ? bwd_first_[g] : 0,
                                    bwd_off_[g + 1] - bwd_off_[g], r, z, split ? 3 : 0, color, active, stream_);
@@ -550,7 +557,8 @@ int BsrSystem::sgs_apply_spmv(const double* r, double* z, double* y, const DotSp
     {
         const double N0 = double(n0) * bs_;
         ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1,
-                     bwd_bytes_[2][groups_bwd() - 1] + double(n0) * b2 * sa + N0 * 8.0 * (1.0 + nx));
+                     bwd_bytes_[2][groups_bwd() - 1] + bwd_blocks_[2][groups_bwd() - 1] * block_bytes() +
+                         double(n0) * b2 * sa + N0 * 8.0 * (1.0 + nx));
         if (mixed) launch_sgs_last_spmv<float>(A, vals32_.p, lu32_.p, n0, z, y, ds, partials, active, stream_);
         else launch_sgs_last_spmv<double>(A, vals64_.p, lu64_.p, n0, z, y, ds, partials, active, stream_);
     }
@@ -966,14 +974,14 @@ void Solver::compute_alg_bytes(int64_t E, int64_t n_c2c, int64_t n_c2f) {
                   ab_.ghost_grad;
     ab_.face_flux = F * (2 * i4 + 4 * d + 3 * d) + visc * F * 4 * d + (n + nb) * (5 + 15 + 5 + 3) * d + F * 6 * d;
     ab_.cell_gather = (n + 1) * i4 + double(n_c2f) * i4 + F * i4 + F * 6 * d + n * 6 * d;
-    const double sa = (cfg_.precision == CFDG_PREC_MIXED) ? 4.0 : 8.0;
     const double b2 = double(nv_) * nv_;
     const double nnzb = sys_ ? double(sys_->nnzb()) : n + 2 * Fi;
     // row-centric assembly: face owner/neigh, normal, area (+ 1/|d|), primitives
     // of cells and ghosts, alpha, CSR cell -> faces, face_pos, diagonal slots,
     // boundary patch ids, the row -> cell map; every block written once
     ab_.jac = F * (2 * i4 + 4 * d + visc * d) + (n + nb) * 5 * d + n * d + (n + 1) * i4 + double(n_c2f) * i4 +
-              Fi * 2 * i4 + n * i4 + nb * i4 + n * i4 + nnzb * b2 * sa;
+              Fi * 2 * i4 + n * i4 + nb * i4 + n * i4;  // + the block stores, at the stored precision
+    ab_.jac_blocks = nnzb * b2;
     ab_.dt_rhs = n * (d * 2 + d * 2 + nv_ * d + 2 * nv_ * d);
     ab_.state_update = n * nv_ * d * 3;
     ab_.norms = n * nv_ * d;
@@ -1406,7 +1414,8 @@ void Solver::assemble_jacobian() {
     js.sa_dsrc = sa_ ? sa_dsrc_.p : nullptr;
     js.cell_of = row_of_h_.empty() ? nullptr : cell_of_.p;
     {
-        ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 1, ab_.jac);
+        ProfScope ps(&prof_, CFDG_KCAT_JACOBIAN, stream_, 1,
+                     ab_.jac + ab_.jac_blocks * (sys_->precision() == CFDG_PREC_MIXED ? 4.0 : 8.0));
         if (sys_->precision() == CFDG_PREC_MIXED)
             launch_jacobian<float>(dm_, df_, gas_, js, nv_, cfg_.viscous != 0, sys_->values32(), stream_);
         else

@@ -203,7 +203,10 @@ private:
     bool lu_ready_ = false;
     std::vector<int32_t> fwd_off_, bwd_off_;
     std::vector<int32_t> fwd_first_, bwd_first_;  // first row of a contiguous group, -1 otherwise
-    std::vector<double> fwd_bytes_[3], bwd_bytes_[3];  // algorithmic bytes of one pass, mode 0 / 1 / split half
+    // algorithmic bytes of one pass, mode 0 / 1 / split half: the part that
+    // does not depend on the matrix precision, and the matrix blocks read
+    std::vector<double> fwd_bytes_[3], bwd_bytes_[3], fwd_blocks_[3], bwd_blocks_[3];
+    double block_bytes() const { return double(bs_) * bs_ * (precision_ == CFDG_PREC_MIXED ? 4.0 : 8.0); }
     bool split_ = false;  // colour-ordered matrix: first sweep split at the diagonal
     DevArray<int32_t> fwd_rows_, bwd_rows_;
     double spmv_bytes(int n_extra_vectors, bool read_y) const;
@@ -331,7 +334,7 @@ private:
     Profiler prof_;
     // algorithmic (unique-touch) bytes per launch of each residual-side kernel
     struct {
-        double prim, grad, limiter, ghost_grad, face_flux, cell_gather, jac, dt_rhs, state_update, norms;
+        double prim, grad, limiter, ghost_grad, face_flux, cell_gather, jac, jac_blocks, dt_rhs, state_update, norms;
         double sa_pre, sa_grad, sa_face;
     } ab_{};
     void compute_alg_bytes(int64_t n_grad_edges, int64_t n_c2c, int64_t n_c2f);
