@@ -45,8 +45,7 @@ void launch_face_flux(const DevMesh& m, const DevFields& f, const GasParams& g, 
 void launch_cell_residual(const DevMesh& m, const DevFields& f, cudaStream_t s);
 int norm_blocks(int32_t n);
 void launch_norms(int32_t n, int nv, const double* res, double* partials, double* l2, cudaStream_t s);
-void launch_dt_rhs(const DevMesh& m, const DevFields& f, int nv, double cfl, double diag, double* b, double* du,
-                   cudaStream_t s);
+void launch_dt_rhs(const DevMesh& m, const DevFields& f, int nv, double cfl, double diag, double* b, cudaStream_t s);
 void launch_unsteady_source(int32_t n, int nv, const double* vol, const double* U, const double* Un,
                             const double* Unm1, double c0, double c1, double c2, double* res, cudaStream_t s);
 void launch_state_update(const DevMesh& m, double* U, const double* du, int nv, cudaStream_t s);

@@ -1,7 +1,7 @@
 // Residual pipeline kernels (Solver::evaluate_residual,
 // include/cfd/solver/compressible/solver.hpp:169-247) and the per-cell
 // time-step / right-hand-side pass (compute_dt solver.hpp:256-287,
-// set_rhs_and_zero_du time/implicit_euler.hpp:81-92).
+// set_rhs_and_zero_du time/implicit_euler.hpp:81-92; du is zeroed in the linear solve).
 //
 // Face-to-cell accumulation is a deterministic cell-centric gather: the
 // face kernel writes each face flux once, the cell kernel sums the fluxes of
@@ -94,7 +94,8 @@ __global__ void __launch_bounds__(128) k_gradient(DevMesh m, const double* __res
 // [n, n+nb) ghosts.
 template <bool LIMIT, int LIM>
 __global__ void __launch_bounds__(128) k_limiter_ghostgrad(DevMesh m, DevFields f, GasParams g, double k3) {
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    // without the limiter (frozen or first order) the grid covers the ghosts only
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x + (LIMIT ? 0 : int64_t(m.n));
     const int64_t n = m.n, nt = m.nt;
     if (t < n) {
         if (!LIMIT) return;
@@ -269,11 +270,13 @@ __global__ void k_norm_finalize(int nblocks, int nv, const double* __restrict__ 
     if (lane == 0) l2[v] = sqrt(s * scale);
 }
 
-// compute_dt (solver.hpp:263-277) fused with set_rhs_and_zero_du
-// (implicit_euler.hpp:81-92): alpha = max(lam,floor)/CFL, b = -R (AoS), du = 0.
+// compute_dt (solver.hpp:263-277) fused with the right-hand side of
+// set_rhs_and_zero_du (implicit_euler.hpp:81-92): alpha = max(lam,floor)/CFL,
+// b = -R (AoS).  The update du starts from zero (or the learned guess) in
+// the linear solve itself.  A 6-variable row of b is 48 bytes and stores as
+// three 16-byte pairs.
 template <int NV>
-__global__ void k_dt_rhs(DevMesh m, DevFields f, double cfl, double diag, double* __restrict__ b,
-                         double* __restrict__ du) {
+__global__ void k_dt_rhs(DevMesh m, DevFields f, double cfl, double diag, double* __restrict__ b) {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.n) return;
     const int64_t n = m.n;
@@ -283,10 +286,16 @@ __global__ void k_dt_rhs(DevMesh m, DevFields f, double cfl, double diag, double
     f.alpha[c] = (l * inv_cfl) + (m.vol[c] * diag);  // diag: BDF coefficient / dt (0 when steady)
     if (b) {
         const int64_t r = row_index(m, c);
+        double v6[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            b[r * NV + v] = -f.res[v * n + c];
-            du[r * NV + v] = 0.0;
+        for (int v = 0; v < NV; ++v) v6[v] = -f.res[v * n + c];
+        if constexpr (NV == 6) {
+            double2* dst = reinterpret_cast<double2*>(b + r * NV);
+#pragma unroll
+            for (int h = 0; h < 3; ++h) dst[h] = make_double2(v6[2 * h], v6[2 * h + 1]);
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) b[r * NV + v] = v6[v];
         }
     }
 }
@@ -335,7 +344,7 @@ void launch_limiter_ghostgrad(const DevMesh& m, const DevFields& f, const GasPar
     const int64_t th = int64_t(m.n) + m.nb;
     const unsigned gr = grid_for(th, 128);
     if (!limit) {
-        k_limiter_ghostgrad<false, 1><<<gr, 128, 0, s>>>(m, f, g, k3);
+        if (m.nb > 0) k_limiter_ghostgrad<false, 1><<<grid_for(m.nb, 128), 128, 0, s>>>(m, f, g, k3);
     } else if (limiter == 2) {
         k_limiter_ghostgrad<true, 2><<<gr, 128, 0, s>>>(m, f, g, k3);
     } else if (limiter == 3) {
@@ -367,11 +376,10 @@ void launch_norms(int32_t n, int nv, const double* res, double* partials, double
     k_norm_finalize<<<1, 32 * 6, 0, s>>>(static_cast<int>(gr), nv, partials, 1.0 / double(n > 0 ? n : 1), l2);
 }
 
-void launch_dt_rhs(const DevMesh& m, const DevFields& f, int nv, double cfl, double diag, double* b, double* du,
-                   cudaStream_t s) {
+void launch_dt_rhs(const DevMesh& m, const DevFields& f, int nv, double cfl, double diag, double* b, cudaStream_t s) {
     const unsigned gr = grid_for(m.n, 256);
-    if (nv == 6) k_dt_rhs<6><<<gr, 256, 0, s>>>(m, f, cfl, diag, b, du);
-    else k_dt_rhs<5><<<gr, 256, 0, s>>>(m, f, cfl, diag, b, du);
+    if (nv == 6) k_dt_rhs<6><<<gr, 256, 0, s>>>(m, f, cfl, diag, b);
+    else k_dt_rhs<5><<<gr, 256, 0, s>>>(m, f, cfl, diag, b);
 }
 
 // Dual-time pseudo-source (Solver::add_unsteady_source_term,

@@ -475,11 +475,13 @@ void BsrSystem::sgs_setup(int ordering, int sweeps) {
     cuda_check(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_), "memset");
     if (precision_ == CFDG_PREC_MIXED) {
         if (!lu32_.p && n_ > 0) alloc_or_throw(lu32_, nb2, "lu");
-        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1, double(n_) * (bs_ * bs_ * 8.0 + bs_ + 4.0));
+        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1,
+                     double(n_) * (bs_ * bs_ * 8.0 + (ordering_ == CFDG_SGS_COLOR ? 0.0 : bs_) + 4.0));
         launch_lu_setup<float>(view(), vals32_.p, lu32_.p, piv_.p, err_.p, ordering_ == CFDG_SGS_COLOR, stream_);
     } else {
         if (!lu64_.p && n_ > 0) alloc_or_throw(lu64_, nb2, "lu");
-        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1, double(n_) * (bs_ * bs_ * 16.0 + bs_ + 4.0));
+        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1,
+                     double(n_) * (bs_ * bs_ * 16.0 + (ordering_ == CFDG_SGS_COLOR ? 0.0 : bs_) + 4.0));
         launch_lu_setup<double>(view(), vals64_.p, lu64_.p, piv_.p, err_.p, ordering_ == CFDG_SGS_COLOR, stream_);
     }
     cuda_check(cudaGetLastError(), "lu launch");
@@ -982,7 +984,7 @@ void Solver::compute_alg_bytes(int64_t E, int64_t n_c2c, int64_t n_c2f) {
     ab_.jac = F * (2 * i4 + 4 * d + visc * d) + (n + nb) * 5 * d + n * d + (n + 1) * i4 + double(n_c2f) * i4 +
               Fi * 2 * i4 + n * i4 + nb * i4 + n * i4;  // + the block stores, at the stored precision
     ab_.jac_blocks = nnzb * b2;
-    ab_.dt_rhs = n * (d * 2 + d * 2 + nv_ * d + 2 * nv_ * d);
+    ab_.dt_rhs = n * (d * 2 + d * 2 + nv_ * d + nv_ * d);  // lam, vol -> dt, alpha; R -> b
     ab_.state_update = n * nv_ * d * 3;
     ab_.norms = n * nv_ * d;
 }
@@ -1398,7 +1400,7 @@ void Solver::compute_dt(double cfl) {
     ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, ab_.dt_rhs);
     // implicit diagonal V/dt_pseudo, plus V c0/dt of the BDF term when unsteady (solver.hpp:267-277)
     const double diag = unsteady_ ? (bdf_cur_ == 2 ? 1.5 : 1.0) / cfg_.dt_physical : 0.0;
-    launch_dt_rhs(dm_, df_, nv_, cfl, diag, b_.p, du_.p, stream_);
+    launch_dt_rhs(dm_, df_, nv_, cfl, diag, b_.p, stream_);
     cuda_check(cudaGetLastError(), "dt launch");
 }
 
