@@ -177,7 +177,7 @@ def _config(case, n, faces, nnzb, args, world, kry=None):
 # direction (profiles/kernels_sa_plate_scale2_fp64.md), 5x5 on the laminar
 # plate divided by 2 (profiles/kernels_plate_scale2_fp64.md).
 TRAFFIC_PER_ALG_BYTE = {"sgs": 262.8 / 236.8, "spmv": 103.1 / 102.0}
-TRAFFIC_PER_ALG_BYTE_SA = {}
+TRAFFIC_PER_ALG_BYTE_SA = {"sgs": 1.016}
 
 
 def _roofline(prof: dict, peak: float, peak_kind: str, traffic_table: dict | None = None):

@@ -283,92 +283,6 @@ __global__ void __launch_bounds__(kLuThreads, 6) k_lu(BsrView A, const MT* __res
     }
 }
 
-// The explicit inverse D^-1 of every diagonal block for the multicolour
-// sweep: a group of BS lanes per block row, lane ii holding row ii of the
-// block and of the inverse being formed (Gauss-Jordan on [D | I] with the
-// partial pivoting of lu_factor_block, bsr_helpers.hpp:278-321: the pivot is
-// the first largest |entry| of column k in rows k..BS-1).  Loads and stores
-// of a group are one contiguous block; 2 x BS doubles of state per lane
-// instead of a whole block and its inverse per thread.
-template <typename MT, int BS>
-__global__ void __launch_bounds__(256) k_inv_groups(BsrView A, const MT* __restrict__ vals, MT* __restrict__ dinv,
-                                                    int* __restrict__ err) {
-    constexpr int GPW = 32 / BS, B2 = BS * BS;
-    const int lane = threadIdx.x & 31;
-    const int grp = lane / BS, ii = lane - grp * BS;
-    const int base = (grp < GPW ? grp : 0) * BS;
-    const int64_t slot = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * GPW + grp;
-    const bool act = grp < GPW && slot < A.n;
-    if (grp >= GPW) return;  // the spare lanes of the warp never join a group
-    const unsigned gmask = ((1u << BS) - 1u) << base;
-    const int32_t i = act ? static_cast<int32_t>(slot) : 0;
-    double a[BS], x[BS];
-    if (act) {
-        const MT* src = vals + int64_t(__ldg(A.diag + i)) * B2 + ii * BS;
-#pragma unroll
-        for (int j = 0; j < BS; ++j) a[j] = ld(src + j);
-    } else {
-#pragma unroll
-        for (int j = 0; j < BS; ++j) a[j] = (j == ii) ? 1.0 : 0.0;
-    }
-#pragma unroll
-    for (int j = 0; j < BS; ++j) x[j] = (j == ii) ? 1.0 : 0.0;
-    bool singular = false;
-#pragma unroll
-    for (int k = 0; k < BS; ++k) {
-        // pivot: first row r >= k with the largest |a[r][k]|
-        int m = k;
-        double mx = fabs(__shfl_sync(gmask, a[k], base + k));
-#pragma unroll
-        for (int r = k + 1; r < BS; ++r) {
-            const double v = fabs(__shfl_sync(gmask, a[k], base + r));
-            if (v > mx) {
-                mx = v;
-                m = r;
-            }
-        }
-        if (mx == 0.0) singular = true;
-        // rows k and m trade places
-#pragma unroll
-        for (int j = 0; j < BS; ++j) {
-            const double ak = __shfl_sync(gmask, a[j], base + k), am = __shfl_sync(gmask, a[j], base + m);
-            const double xk = __shfl_sync(gmask, x[j], base + k), xm = __shfl_sync(gmask, x[j], base + m);
-            if (ii == k) {
-                a[j] = am;
-                x[j] = xm;
-            } else if (ii == m) {
-                a[j] = ak;
-                x[j] = xk;
-            }
-        }
-        // eliminate column k from every other row, scale the pivot row
-        const double inv_d = 1.0 / __shfl_sync(gmask, a[k], base + k);
-        const double l = a[k] * inv_d;
-#pragma unroll
-        for (int j = 0; j < BS; ++j) {
-            const double pa = __shfl_sync(gmask, a[j], base + k), px = __shfl_sync(gmask, x[j], base + k);
-            if (ii == k) {
-                a[j] = pa * inv_d;
-                x[j] = px * inv_d;
-            } else {
-                a[j] -= l * pa;
-                x[j] -= l * px;
-            }
-        }
-    }
-    if (!act) return;
-    MT* dst = dinv + int64_t(i) * B2 + ii * BS;
-    bool finite = true;
-#pragma unroll
-    for (int j = 0; j < BS; ++j) {
-        dst[j] = static_cast<MT>(x[j]);
-        finite = finite && isfinite(x[j]);
-    }
-    // +(i+1): zero pivot (singular block); -(i+1): non-finite entries
-    if (singular) atomicCAS(err, 0, i + 1);
-    else if (!finite) atomicCAS(err, 0, -(i + 1));
-}
-
 // Pivoted forward/backward substitution of one block (lu_solve_block) in
 // registers; b holds the right-hand side on entry and the solution on exit.
 template <typename MT, int BS, bool SMEM = false>
@@ -811,9 +725,8 @@ template <typename MT>
 void launch_lu_setup(const BsrView& A, const MT* vals, MT* lu, int8_t* piv, int* err_flag, bool inverse,
                      cudaStream_t s) {
     const unsigned gr = grid_for(A.n, kLuThreads);
-    const unsigned gi = grid_for((int64_t(A.n) + 32 / A.bs - 1) / (32 / A.bs) * 32, 256);
-#define CFDG_LU(BS)                                                                      \
-    if (inverse) k_inv_groups<MT, BS><<<gi, 256, 0, s>>>(A, vals, lu, err_flag);        \
+#define CFDG_LU(BS)                                                                          \
+    if (inverse) k_lu<MT, BS, true><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag); \
     else k_lu<MT, BS, false><<<gr, kLuThreads, 0, s>>>(A, vals, lu, piv, err_flag)
     switch (A.bs) {
         case 1: CFDG_LU(1); break;

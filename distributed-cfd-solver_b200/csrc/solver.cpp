@@ -475,13 +475,11 @@ void BsrSystem::sgs_setup(int ordering, int sweeps) {
     cuda_check(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_), "memset");
     if (precision_ == CFDG_PREC_MIXED) {
         if (!lu32_.p && n_ > 0) alloc_or_throw(lu32_, nb2, "lu");
-        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1,
-                     double(n_) * (bs_ * bs_ * 8.0 + (ordering_ == CFDG_SGS_COLOR ? 0.0 : bs_) + 4.0));
+        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1, double(n_) * (bs_ * bs_ * 8.0 + bs_ + 4.0));
         launch_lu_setup<float>(view(), vals32_.p, lu32_.p, piv_.p, err_.p, ordering_ == CFDG_SGS_COLOR, stream_);
     } else {
         if (!lu64_.p && n_ > 0) alloc_or_throw(lu64_, nb2, "lu");
-        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1,
-                     double(n_) * (bs_ * bs_ * 16.0 + (ordering_ == CFDG_SGS_COLOR ? 0.0 : bs_) + 4.0));
+        ProfScope ps(prof_, CFDG_KCAT_LU, stream_, 1, double(n_) * (bs_ * bs_ * 16.0 + bs_ + 4.0));
         launch_lu_setup<double>(view(), vals64_.p, lu64_.p, piv_.p, err_.p, ordering_ == CFDG_SGS_COLOR, stream_);
     }
     cuda_check(cudaGetLastError(), "lu launch");
