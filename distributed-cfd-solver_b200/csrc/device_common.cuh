@@ -60,7 +60,7 @@ struct DevFields {
     double* q;       // 5 * nt
     double* grad;    // nv_grad * 3 * nt
     double* phi;     // 5 * n
-    double* fflux;   // (nv + 1) * nf: face flux per variable, then A*s_max
+    double* fflux;   // 6 * nf, face-major: the 5 face fluxes then A*s_max of face f at fflux + 6 f
     double* res;     // nv * n
     double* lam;     // n
     double* dt;      // n

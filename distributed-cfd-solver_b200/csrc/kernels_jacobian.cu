@@ -152,8 +152,12 @@ __device__ __forceinline__ double visc_entry(const ViscFace& v, const GasParams&
     return -v.cl * u[c - 1] * v.inv_rho_cv + v.cm * v.Mu[c - 1] * v.inv_rho;
 }
 
+// 4 blocks of 128 threads per SM (128 registers), 3 for the viscous rows,
+// whose per-thread state (the viscous face terms on top of the Euler
+// ones) spills at 128 registers.
 template <typename MT, bool VISC, int BS, bool FULL>
-__global__ void __launch_bounds__(128, 4) k_jac_rows(DevMesh m, DevFields f, GasParams g, JacStructure js, MT* vals) {
+__global__ void __launch_bounds__(128, VISC ? 3 : 4)
+    k_jac_rows(DevMesh m, DevFields f, GasParams g, JacStructure js, MT* vals) {
     __shared__ MT stage_all[4][32][stage_stride<BS>()];
     MT(*stage)[stage_stride<BS>()] = stage_all[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;

@@ -168,8 +168,10 @@ constexpr int kLuThreads = 128;
 // INV: the factors are used once more to form the explicit inverse D^-1
 // (A x = e_c column by column), which is stored instead of the factors; the
 // multicolour sweep then applies D^-1 as a block-row product.
+// Occupancy bound per block size: the 6x6 factor, pivots and inverse
+// column of a thread spill below ~170 registers, the 5x5 ones below ~128.
 template <typename MT, int BS, bool INV>
-__global__ void __launch_bounds__(kLuThreads, 6) k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu,
+__global__ void __launch_bounds__(kLuThreads, BS == 6 ? 3 : 4) k_lu(BsrView A, const MT* __restrict__ vals, MT* __restrict__ lu,
                                                    int8_t* __restrict__ piv, int* __restrict__ err) {
     constexpr int B2 = BS * BS;
     constexpr int SP = B2 % 2 == 0 ? B2 + 1 : B2;  // odd row stride: thread-per-row accesses hit distinct banks

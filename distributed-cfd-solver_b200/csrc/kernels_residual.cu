@@ -161,7 +161,7 @@ template <bool MUSCL, bool VISC>
 __global__ void __launch_bounds__(128, VISC ? 0 : 6) k_face_flux(DevMesh m, DevFields f, GasParams g) {
     const int32_t fc = blockIdx.x * blockDim.x + threadIdx.x;
     if (fc >= m.nf) return;
-    const int64_t nt = m.nt, nf = m.nf;
+    const int64_t nt = m.nt;
     const bool inner = fc < m.ni;
     const int32_t c0 = m.owner[fc];
     const int32_t c1 = inner ? m.neigh[fc] : m.n + (fc - m.ni);
@@ -215,28 +215,33 @@ __global__ void __launch_bounds__(128, VISC ? 0 : 6) k_face_flux(DevMesh m, DevF
         for (int v = 1; v < 5; ++v) F[v] += Fv[v];
         lam_f += lv;
     }
-#pragma unroll
-    for (int v = 0; v < 5; ++v) f.fflux[v * nf + fc] = F[v];
-    f.fflux[5 * nf + fc] = lam_f;
+    // face-major: the face's 5 fluxes and A*s_max are one 48-byte record
+    double2* dst = reinterpret_cast<double2*>(f.fflux + int64_t(fc) * 6);
+    dst[0] = make_double2(F[0], F[1]);
+    dst[1] = make_double2(F[2], F[3]);
+    dst[2] = make_double2(F[4], lam_f);
 }
 
 // Cell gather of face fluxes into R and lam (ascending face order).
 __global__ void __launch_bounds__(256) k_cell_residual(DevMesh m, DevFields f) {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.n) return;
-    const int64_t nf = m.nf, n = m.n;
+    const int64_t n = m.n;
     double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double l = 0.0;
     for (int32_t e = m.c2f_off[c]; e < m.c2f_off[c + 1]; ++e) {
         const int32_t fc = m.c2f[e];
+        const double2* rec = reinterpret_cast<const double2*>(f.fflux + int64_t(fc) * 6);
+        const double2 a = __ldg(rec), b = __ldg(rec + 1), d = __ldg(rec + 2);
+        const double F[5] = {a.x, a.y, b.x, b.y, d.x};
         if (m.owner[fc] == c) {
 #pragma unroll
-            for (int v = 0; v < 5; ++v) r[v] += f.fflux[v * nf + fc];
+            for (int v = 0; v < 5; ++v) r[v] += F[v];
         } else {
 #pragma unroll
-            for (int v = 0; v < 5; ++v) r[v] -= f.fflux[v * nf + fc];
+            for (int v = 0; v < 5; ++v) r[v] -= F[v];
         }
-        l += f.fflux[5 * nf + fc];
+        l += d.y;
     }
 #pragma unroll
     for (int v = 0; v < 5; ++v) f.res[v * n + c] = r[v];

@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(128) k_sa_face(DevMesh m, DevFields f, GasPara
     const int32_t c0 = m.owner[fc];
     const int64_t c1 = inner ? m.neigh[fc] : int64_t(m.n) + (fc - m.ni);
     const double nx = m.fnx[fc], ny = m.fny[fc], nz = m.fnz[fc], A = m.farea[fc];
-    const double mf = f.fflux[fc];  // mass flux of the mean-flow sweep (row 0)
+    const double mf = f.fflux[int64_t(fc) * 6];  // mass flux of the mean-flow sweep (entry 0 of the face record)
     const double is = 1.0 / sa.sigma;
     const double dx = m.fdx[fc], dy = m.fdy[fc], dz = m.fdz[fc], id = m.finv_d[fc];
     const double nu0 = f.nu[c0];
