@@ -71,8 +71,8 @@ struct JacStructure {
     const int32_t* diag;      // n
     const int32_t* face_pos;  // 2*ni: block (owner,neigh), block (neigh,owner)
     bool full_viscous;        // thin-layer operator with the normal-stress term + no-slip ghost
-    // Spalart-Allmaras (6x6 blocks): per face d(nu_tilde flux)/d(rho nu_tilde)
-    // of owner [0, nf) and neighbour [nf, 2 nf), and the destruction
+    // Spalart-Allmaras (6x6 blocks): per face the pair d(nu_tilde flux)/d(rho
+    // nu_tilde) of owner and neighbour at [2f, 2f+1], and the destruction
     // derivative per cell; null without the model
     const double* sa_jac;
     const double* sa_dsrc;

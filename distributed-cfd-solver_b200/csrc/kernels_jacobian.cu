@@ -236,8 +236,9 @@ __global__ void __launch_bounds__(128, VISC ? 3 : 4)
                     stage[lane][k * BS + 5] = MT(0);
                     stage[lane][5 * BS + k] = MT(0);
                 }
-                stage[lane][BS * BS - 1] = to_mt<MT>(own ? js.sa_jac[m.nf + fc] : -js.sa_jac[fc]);
-                d35 += own ? js.sa_jac[fc] : -js.sa_jac[m.nf + fc];
+                const double2 sj = reinterpret_cast<const double2*>(js.sa_jac)[fc];  // owner, neighbour
+                stage[lane][BS * BS - 1] = to_mt<MT>(own ? sj.y : -sj.x);
+                d35 += own ? sj.x : -sj.y;
             }
             pos = js.face_pos[2 * fc + (own ? 0 : 1)];
         } else if (has) {
@@ -265,7 +266,7 @@ __global__ void __launch_bounds__(128, VISC ? 3 : 4)
                     if (VISC) d1 += visc_entry<FULL>(vf, g, nx, ny, nz, rr, cc);
                     D[rr * 5 + cc] += d1;
                 }
-            if (BS == 6) d35 += js.sa_jac[fc];
+            if (BS == 6) d35 += js.sa_jac[2 * int64_t(fc)];
         }
         warp_store_blocks<MT, BS>(stage, pos, inner, vals);
     }

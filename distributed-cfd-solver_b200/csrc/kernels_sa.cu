@@ -52,9 +52,11 @@ __global__ void k_sa_pre(DevMesh m, DevFields f, GasParams g, SaParams sa, doubl
 }
 
 // Face sweep (SpalartAllmaras::face_sweep, spalart_allmaras.hpp:291-368):
-// out[f] = convective - diffusive nu_tilde flux, out[nf+f] = spectral-radius
-// increment (interior faces), jac[f] / jac[nf+f] = d flux / d(rho nu_tilde)
-// of owner / neighbour (boundary faces: owner incl. the ghost's dependence).
+// Face-major pairs: out[2f] = convective - diffusive nu_tilde flux,
+// out[2f+1] = spectral-radius increment (interior faces); jac[2f] /
+// jac[2f+1] = d flux / d(rho nu_tilde) of owner / neighbour (boundary
+// faces: owner incl. the ghost's dependence).  A cell's gather then reads
+// one 16-byte pair per face.
 __global__ void __launch_bounds__(128) k_sa_face(DevMesh m, DevFields f, GasParams g, SaParams sa,
                                                  const double* __restrict__ rhonu_g, const double* __restrict__ gnu,
                                                  double* __restrict__ out, double* __restrict__ jac) {
@@ -114,16 +116,14 @@ __global__ void __launch_bounds__(128) k_sa_face(DevMesh m, DevFields f, GasPara
     double nu_up;
     if (inner) nu_up = (mf >= 0.0) ? nu0 : nu1;
     else nu_up = inflow ? sa.nu_inf : nu0;
-    out[fc] = mf * nu_up - fd;
-    out[nf + fc] = inner ? (fabs(mf) / rho_f + 2.0 * is * (mu_f + rho_f * (0.5 * (nu0 + nu1))) / rho_f * A * id) : 0.0;
+    const double lam_inc =
+        inner ? (fabs(mf) / rho_f + 2.0 * is * (mu_f + rho_f * (0.5 * (nu0 + nu1))) / rho_f * A * id) : 0.0;
+    reinterpret_cast<double2*>(out)[fc] = make_double2(mf * nu_up - fd, lam_inc);
     const double cd = coef * A * id;
-    if (inner) {
-        jac[fc] = (fmax(mf, 0.0) + cd) / rho0;
-        jac[nf + fc] = (fmin(mf, 0.0) - cd) / rho1;
-    } else {
-        jac[fc] = (inflow ? 0.0 : mf / rho0) + cd * (1.0 / rho0 - dg);
-        jac[nf + fc] = 0.0;
-    }
+    if (inner)
+        reinterpret_cast<double2*>(jac)[fc] = make_double2((fmax(mf, 0.0) + cd) / rho0, (fmin(mf, 0.0) - cd) / rho1);
+    else
+        reinterpret_cast<double2*>(jac)[fc] = make_double2((inflow ? 0.0 : mf / rho0) + cd * (1.0 / rho0 - dg), 0.0);
 }
 
 // Cell gather of the nu_tilde fluxes (ascending face order, as the
@@ -134,13 +134,14 @@ __global__ void __launch_bounds__(128) k_sa_cell(DevMesh m, DevFields f, SaParam
                                                  const double* __restrict__ gnu, double* __restrict__ dsrc) {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.n) return;
-    const int64_t nt = m.nt, nf = m.nf, n = m.n;
+    const int64_t nt = m.nt, n = m.n;
     double r = 0.0, l = f.lam[c];
     for (int32_t e = m.c2f_off[c]; e < m.c2f_off[c + 1]; ++e) {
         const int32_t fc = m.c2f[e];
-        if (m.owner[fc] == c) r += face[fc];
-        else r -= face[fc];
-        if (fc < m.ni) l += face[nf + fc];
+        const double2 fr = __ldg(reinterpret_cast<const double2*>(face) + fc);
+        if (m.owner[fc] == c) r += fr.x;
+        else r -= fr.x;
+        if (fc < m.ni) l += fr.y;
     }
     f.lam[c] = l;
     const double rho = f.rho[c], nu = f.nu[c];
