@@ -48,9 +48,10 @@ JAC_REFERENCE, JAC_THIN_LAYER = 0, 1
 KRYLOV_DEVICE_LOOP, KRYLOV_HOST_LOOP = 0, 1
 PREFREEZE_CONFIGURED, PREFREEZE_FP64 = 0, 1
 TIME_STEADY, TIME_UNSTEADY = 0, 1
+NEWTON_PICARD, NEWTON_JACOBIAN_FREE = 0, 1
 STAGE_PRIMITIVES, STAGE_GRADIENT, STAGE_LIMITER, STAGE_FLUXES = range(4)
 KCAT_NAMES = ("primitives", "gradient", "limiter", "face_flux", "cell_gather", "jacobian", "lu", "spmv", "sgs",
-              "krylov", "update", "turbulence", "guess")
+              "krylov", "update", "turbulence", "guess", "jfnk")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -93,7 +94,9 @@ class Config(C.Structure):
                 ("cfl_max", C.c_double), ("residual_tolerance", C.c_double), ("lin_rel_tol", C.c_double),
                 ("lin_abs_tol", C.c_double), ("nu_inf_ratio", C.c_double), ("max_iterations", C.c_int64),
                 ("dt_physical", C.c_double), ("max_time_steps", C.c_int64), ("time_mode", C.c_int32),
-                ("bdf_order", C.c_int32)]
+                ("bdf_order", C.c_int32), ("newton_operator", C.c_int32), ("jf_max_iterations", C.c_int32),
+                ("jf_rel_tol", C.c_double), ("jf_eps", C.c_double), ("jf_max_change", C.c_double),
+                ("cfl_ser_max", C.c_double)]
 
 
 class UnsteadyResult(C.Structure):
@@ -110,13 +113,15 @@ class KrylovResult(C.Structure):
 class StepResult(C.Structure):
     _fields_ = [("l2", C.c_double * 6), ("cfl", C.c_double), ("nvars", C.c_int32), ("krylov_status", C.c_int32),
                 ("krylov_iterations", C.c_int32), ("guess_used", C.c_int32), ("krylov_initial", C.c_double),
-                ("krylov_final", C.c_double), ("krylov_rhs", C.c_double)]
+                ("krylov_final", C.c_double), ("krylov_rhs", C.c_double), ("jacobian_free", C.c_int32),
+                ("picard_fallback", C.c_int32), ("step_scale", C.c_double)]
 
 
 class RunResult(C.Structure):
     _fields_ = [("iterations", C.c_int64), ("converged", C.c_int32), ("blowup", C.c_int32), ("rel", C.c_double),
                 ("seconds", C.c_double), ("krylov_iterations_total", C.c_int64), ("l2_first", C.c_double * 6),
-                ("l2_last", C.c_double * 6)]
+                ("l2_last", C.c_double * 6), ("jacobian_free_steps", C.c_int64), ("picard_fallbacks", C.c_int64),
+                ("cfl_last", C.c_double)]
 
 
 class MeshSpec(C.Structure):
@@ -253,7 +258,9 @@ CONFIG_DEFAULTS = dict(
     gamma=1.4, gas_constant=287.052874, prandtl=0.71, prandtl_turb=0.9, init_rho=1.225, init_p=101325.0,
     init_velocity=(0.0, 0.0, 0.0), venkat_k=0.5, cfl=0.4, cfl_max=0.4, residual_tolerance=1.0e-10,
     lin_rel_tol=1.0e-1, lin_abs_tol=1.0e-15, nu_inf_ratio=3.0, max_iterations=10000,
-    dt_physical=1.0e-6, max_time_steps=1, time_mode=TIME_STEADY, bdf_order=2)
+    dt_physical=1.0e-6, max_time_steps=1, time_mode=TIME_STEADY, bdf_order=2,
+    newton_operator=NEWTON_PICARD, jf_max_iterations=60, jf_rel_tol=1.0e-2, jf_eps=1.0e-7, jf_max_change=0.2,
+    cfl_ser_max=0.0)
 
 
 def default_config(**overrides) -> Config:

@@ -152,6 +152,12 @@ void cfdg_config_default(cfdg_config* c) {
     c->max_time_steps = 1;
     c->time_mode = CFDG_TIME_STEADY;
     c->bdf_order = 2;
+    c->newton_operator = CFDG_NEWTON_PICARD;
+    c->jf_max_iterations = 60;
+    c->jf_rel_tol = 1.0e-2;
+    c->jf_eps = 1.0e-7;
+    c->jf_max_change = 0.2;
+    c->cfl_ser_max = 0.0;
 }
 
 // ------------------------------------------------------------------ meshes

@@ -48,7 +48,7 @@ void launch_norms(int32_t n, int nv, const double* res, double* partials, double
 void launch_dt_rhs(const DevMesh& m, const DevFields& f, int nv, double cfl, double diag, double* b, cudaStream_t s);
 void launch_unsteady_source(int32_t n, int nv, const double* vol, const double* U, const double* Un,
                             const double* Unm1, double c0, double c1, double c2, double* res, cudaStream_t s);
-void launch_state_update(const DevMesh& m, double* U, const double* du, int nv, cudaStream_t s);
+void launch_state_update(const DevMesh& m, double* U, const double* du, int nv, const double* scale, cudaStream_t s);
 void launch_fill(double* x, int64_t count, double value, cudaStream_t s);
 
 // -------------------------------------------------------- Spalart-Allmaras
@@ -82,6 +82,20 @@ template <typename MT>
 void launch_jacobian(const DevMesh& m, const DevFields& f, const GasParams& g, const JacStructure& js, int bs,
                      bool visc, MT* values, cudaStream_t s);
 
+
+// ------------------------------------------- Jacobian-free Newton-Krylov
+// Device scalars of the Jacobian-free product (a buffer of kJfScalars
+// doubles): [0, nv) RMS of each conserved variable, then the product's step
+// length and the Newton step's relaxation factor.
+enum : int { kJfEps = 6, kJfStep = 7, kJfScalars = 16 };
+int jf_partial_blocks(int32_t n);  // partial rows of the reductions below (x nv doubles)
+void launch_jf_rms(int32_t n, int nv, const double* U, double* partials, double* scal, cudaStream_t s);
+void launch_jf_eps(int32_t rows, int nv, const double* x, double* partials, double* scal, double eps_rel,
+                   const int* active, cudaStream_t s);
+void launch_jf_perturb(const DevMesh& m, int nv, const double* U, const double* x, const double* scal, double* Up,
+                       const int* active, cudaStream_t s);
+void launch_jf_step_scale(const DevMesh& m, int nv, const double* U, const double* du, double* partials, double* scal,
+                          double max_change, cudaStream_t s);
 
 // ------------------------------------------------------------ linear algebra
 struct BsrView {

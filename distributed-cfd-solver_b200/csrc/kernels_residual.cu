@@ -306,16 +306,19 @@ __global__ void k_dt_rhs(DevMesh m, DevFields f, double cfl, double diag, double
 }
 
 // U <- U + du (AoS du), implicit_euler.hpp:49-61; SA variable clamped at 0
-// (SpalartAllmaras::post_stage).
+// (SpalartAllmaras::post_stage).  `scale` (device scalar, may be null):
+// U <- U + scale * du, the relaxed Jacobian-free step.
 template <int NV>
-__global__ void k_state_update(DevMesh m, double* __restrict__ U, const double* __restrict__ du) {
+__global__ void k_state_update(DevMesh m, double* __restrict__ U, const double* __restrict__ du,
+                               const double* __restrict__ scale) {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.n) return;
     const int64_t n = m.n;
     const int64_t r = row_index(m, c);
+    const double w = scale ? *scale : 1.0;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        double x = U[v * n + c] + du[r * NV + v];
+        double x = scale ? U[v * n + c] + w * du[r * NV + v] : U[v * n + c] + du[r * NV + v];
         if (v == 5 && x < 0.0) x = 0.0;
         U[v * n + c] = x;
     }
@@ -406,10 +409,10 @@ void launch_unsteady_source(int32_t n, int nv, const double* vol, const double* 
     if (len > 0) k_unsteady_source<<<grid_for(len, 256), 256, 0, s>>>(n, nv, vol, U, Un, Unm1, c0, c1, c2, res);
 }
 
-void launch_state_update(const DevMesh& m, double* U, const double* du, int nv, cudaStream_t s) {
+void launch_state_update(const DevMesh& m, double* U, const double* du, int nv, const double* scale, cudaStream_t s) {
     const unsigned gr = grid_for(m.n, 256);
-    if (nv == 6) k_state_update<6><<<gr, 256, 0, s>>>(m, U, du);
-    else k_state_update<5><<<gr, 256, 0, s>>>(m, U, du);
+    if (nv == 6) k_state_update<6><<<gr, 256, 0, s>>>(m, U, du, scale);
+    else k_state_update<5><<<gr, 256, 0, s>>>(m, U, du, scale);
 }
 
 void launch_fill(double* x, int64_t count, double value, cudaStream_t s) {

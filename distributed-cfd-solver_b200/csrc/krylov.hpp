@@ -31,6 +31,13 @@ struct DotSpec {
     int n;
 };
 
+// Jacobian-free product y = (alpha - V diag) x + (R(U + eps x) + b) / eps
+// from the perturbed residual `resp` (SoA, cell order), with the dots `ds`;
+// returns the partial count.
+int launch_jf_combine(const DevMesh& m, int nv, const double* alpha, double diag, const double* x, const double* b,
+                      const double* resp, const double* scal, double* y, const DotSpec& ds, double* partials,
+                      const int* active, cudaStream_t s);
+
 // y = alpha A x + beta y on rows [row_begin, n), optional fused dots
 template <typename MT>
 void launch_spmv_ex(const BsrView& A, const MT* vals, const double* x, double* y, double alpha, double beta,

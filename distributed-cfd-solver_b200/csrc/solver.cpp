@@ -649,16 +649,27 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
     init.guess = guess ? 1 : 0;
     cuda_check(cudaMemcpyAsync(ks_.p, &init, sizeof(init), cudaMemcpyHostToDevice, stream_), "H2D");
     const int* active = &ks_.p->state;
-    auto spmv_dots = [&](const double* xin, double* yout, const DotSpec& ds) {
+    const bool matrix_free = static_cast<bool>(product_);
+    // y = A x (or the matrix-free product) with the dots ds; returns the partial rows
+    auto spmv_dots = [&](const double* xin, double* yout, const DotSpec& ds) -> int {
+        if (matrix_free) return product_(xin, yout, ds, partials_.p, active);
         ProfScope ps(prof_, CFDG_KCAT_SPMV, stream_, 1, spmv_bytes(ds.n == 1 ? 1 : 2, false));
         if (mixed) launch_spmv_ex<float>(A, vals32_.p, xin, yout, 1.0, 0.0, ds, partials_.p, active, stream_);
         else launch_spmv_ex<double>(A, vals64_.p, xin, yout, 1.0, 0.0, ds, partials_.p, active, stream_);
+        return spmv_blocks(n_, bs_);
     };
     // r = b - A x; r0 = r; p = r
     {
         DotSpec none{};
         none.n = 0;
-        {
+        if (matrix_free) {
+            if (guess) {
+                product_(x, v_.p, none, nullptr, nullptr);
+            } else {  // x = 0: A x = 0 without a residual evaluation
+                ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 1, 8.0 * N);
+                cuda_check(cudaMemsetAsync(v_.p, 0, sizeof(double) * N, stream_), "memset");
+            }
+        } else {
             ProfScope ps(prof_, CFDG_KCAT_SPMV, stream_, 1, spmv_bytes(0, false));
             if (mixed) launch_spmv_ex<float>(A, vals32_.p, x, v_.p, 1.0, 0.0, none, nullptr, nullptr, stream_);
             else launch_spmv_ex<double>(A, vals64_.p, x, v_.p, 1.0, 0.0, none, nullptr, nullptr, stream_);
@@ -685,11 +696,15 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
         d1.b[0] = nullptr;
         double* phat = p_.p;
         int nb1 = nblk;
-        if (precond == CFDG_PC_SGS) {
+        if (precond == CFDG_PC_SGS && matrix_free) {
+            sgs_apply(p_.p, phat_.p, active);
+            phat = phat_.p;
+            nb1 = spmv_dots(phat, v_.p, d1);
+        } else if (precond == CFDG_PC_SGS) {
             nb1 = sgs_apply_spmv(p_.p, phat_.p, v_.p, d1, partials_.p, active);
             phat = phat_.p;
         } else {
-            spmv_dots(phat, v_.p, d1);
+            nb1 = spmv_dots(phat, v_.p, d1);
         }
         {
             ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 2, 3.0 * 8.0 * N);
@@ -705,11 +720,15 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
         d5.a[4] = s_.p;    d5.b[4] = s_.p;      // s.s
         double* shat = s_.p;
         int nb5 = nblk;
-        if (precond == CFDG_PC_SGS) {
+        if (precond == CFDG_PC_SGS && matrix_free) {
+            sgs_apply(s_.p, shat_.p, active);
+            shat = shat_.p;
+            nb5 = spmv_dots(shat, t_.p, d5);
+        } else if (precond == CFDG_PC_SGS) {
             nb5 = sgs_apply_spmv(s_.p, shat_.p, t_.p, d5, partials_.p, active);
             shat = shat_.p;
         } else {
-            spmv_dots(shat, t_.p, d5);
+            nb5 = spmv_dots(shat, t_.p, d5);
         }
         {
             ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 3, 10.0 * 8.0 * N);
@@ -718,7 +737,7 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
             launch_krylov_post(ks_.p, partials_.p, nvec, stream_);
         }
     };
-    if (device_loop && !prof_->on() && max_it > 0 && device_loop_ready(precond, x, b, iteration)) {
+    if (device_loop && !matrix_free && !prof_->on() && max_it > 0 && device_loop_ready(precond, x, b, iteration)) {
         cuda_check(cudaGraphLaunch(loop_exec_, stream_), "krylov graph launch");
         cuda_check(cudaMemcpyAsync(ks_host_, ks_.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, stream_), "D2H");
         cuda_check(cudaStreamSynchronize(stream_), "krylov sync");
@@ -781,6 +800,12 @@ Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, c
         throw Failure{CFDG_ERR_INVALID, "unknown pre-freeze mode"};
     if (cfg.time_mode != CFDG_TIME_STEADY && cfg.time_mode != CFDG_TIME_UNSTEADY)
         throw Failure{CFDG_ERR_INVALID, "unknown time mode"};
+    if (cfg.newton_operator != CFDG_NEWTON_PICARD && cfg.newton_operator != CFDG_NEWTON_JACOBIAN_FREE)
+        throw Failure{CFDG_ERR_INVALID, "unknown Newton operator"};
+    if (cfg.newton_operator == CFDG_NEWTON_JACOBIAN_FREE &&
+        (!(cfg.jf_eps > 0.0) || !(cfg.jf_rel_tol > 0.0) || cfg.jf_max_iterations < 1 || !(cfg.jf_max_change >= 0.0)))
+        throw Failure{CFDG_ERR_INVALID,
+                      "Jacobian-free Newton needs jf_eps > 0, jf_rel_tol > 0, jf_max_iterations >= 1, jf_max_change >= 0"};
     unsteady_ = cfg.time_mode == CFDG_TIME_UNSTEADY;
     if (unsteady_ && (cfg.bdf_order < 1 || cfg.bdf_order > 2 || !(cfg.dt_physical > 0.0) || cfg.max_time_steps < 0))
         throw Failure{CFDG_ERR_INVALID, "unsteady mode needs bdf_order 1 or 2, dt_physical > 0, max_time_steps >= 0"};
@@ -823,6 +848,7 @@ Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, c
 
 Solver::~Solver() {
     if (l2_host_) cudaFreeHost(l2_host_);
+    if (jf_host_) cudaFreeHost(jf_host_);
     sys_.reset();
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -1374,9 +1400,9 @@ void Solver::stage(int st) {
                 const bool bdf2 = bdf_cur_ == 2;
                 const double n = double(dm_.n) * nv_;
                 ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, n * 8.0 * (bdf2 ? 5.0 : 4.0) + dm_.n * 8.0);
-                launch_unsteady_source(dm_.n, nv_, vol_.p, U_.p, Un_.p, bdf2 ? Unm1_.p : nullptr,
+                launch_unsteady_source(dm_.n, nv_, vol_.p, df_.U, Un_.p, bdf2 ? Unm1_.p : nullptr,
                                        (bdf2 ? 1.5 : 1.0) * idt, (bdf2 ? -2.0 : -1.0) * idt, bdf2 ? 0.5 * idt : 0.0,
-                                       res_.p, stream_);
+                                       df_.res, stream_);
             }
             break;
         }
@@ -1438,10 +1464,87 @@ cfdg_krylov_result Solver::linear_solve() {
     } else {
         cuda_check(cudaMemsetAsync(du_.p, 0, du_.count * sizeof(double), stream_), "memset");
     }
-    last_krylov_ = sys_->bicgstab(cfg_.precond, cfg_.lin_rel_tol, cfg_.lin_abs_tol, cfg_.lin_max_iterations, du_.p,
-                                  b_.p, use_guess);
+    last_jf_ = last_fallback_ = false;
     last_used_guess_ = use_guess;
+    if (!jf_now()) {
+        last_krylov_ = sys_->bicgstab(cfg_.precond, cfg_.lin_rel_tol, cfg_.lin_abs_tol, cfg_.lin_max_iterations,
+                                      du_.p, b_.p, use_guess);
+        return last_krylov_;
+    }
+    // Jacobian-free solve, replaced by the Picard solve when it does not
+    // reduce its residual
+    jf_alloc();
+    {
+        ProfScope ps(&prof_, CFDG_KCAT_JFNK, stream_, 2, double(dm_.n) * nv_ * 8.0);
+        launch_jf_rms(dm_.n, nv_, U_.p, jf_part_.p, jf_scal_.p, stream_);
+    }
+    sys_->set_product([this](const double* x, double* y, const DotSpec& ds, double* partials, const int* active) {
+        return jf_product(x, y, ds, partials, active);
+    });
+    cfdg_krylov_result kr{};
+    try {
+        kr = sys_->bicgstab(cfg_.precond, cfg_.jf_rel_tol, cfg_.lin_abs_tol, cfg_.jf_max_iterations, du_.p, b_.p,
+                            use_guess);
+    } catch (...) {
+        sys_->set_product(nullptr);
+        throw;
+    }
+    sys_->set_product(nullptr);
+    const double bnorm = sys_->last_bnorm();
+    if (kr.status != CFDG_KRYLOV_DIVERGED && std::isfinite(kr.final_residual) && kr.final_residual < bnorm) {
+        last_jf_ = true;
+        last_krylov_ = kr;
+        return last_krylov_;
+    }
+    cuda_check(cudaMemsetAsync(du_.p, 0, du_.count * sizeof(double), stream_), "memset");
+    cfdg_krylov_result pk = sys_->bicgstab(cfg_.precond, cfg_.lin_rel_tol, cfg_.lin_abs_tol,
+                                           cfg_.lin_max_iterations, du_.p, b_.p, false);
+    pk.iterations += kr.iterations;
+    last_fallback_ = true;
+    last_used_guess_ = false;
+    last_krylov_ = pk;
     return last_krylov_;
+}
+
+void Solver::jf_alloc() {
+    if (jf_U_.p) return;
+    const std::size_t n = static_cast<std::size_t>(dm_.n);
+    alloc_or_throw(jf_U_, n * nv_, "perturbed state");
+    alloc_or_throw(jf_res_, n * nv_, "perturbed residual");
+    alloc_or_throw(jf_part_, static_cast<std::size_t>(jf_partial_blocks(dm_.n)) * 6 + 8, "product partials");
+    alloc_or_throw(jf_scal_, kJfScalars, "product scalars");
+    cuda_check(cudaMemsetAsync(jf_scal_.p, 0, kJfScalars * sizeof(double), stream_), "memset");
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&jf_host_), sizeof(double) * 8), "cudaMallocHost");
+}
+
+// y = (V/dt) x + (R(U + eps x) - R(U)) / eps: the residual stages run on the
+// perturbed state with the perturbed residual in its own buffer (R(U) stays
+// in res_ and -R(U) in b_); the primitives, gradients and face fluxes are
+// overwritten and recomputed at the next evaluation.
+int Solver::jf_product(const double* x, double* y, const DotSpec& ds, double* partials, const int* active) {
+    const double N = double(dm_.n) * nv_;
+    {
+        ProfScope ps(&prof_, CFDG_KCAT_JFNK, stream_, 3, N * 8.0 * 4.0 + double(dm_.n) * 4.0);
+        launch_jf_eps(dm_.n, nv_, x, jf_part_.p, jf_scal_.p, cfg_.jf_eps, active, stream_);
+        launch_jf_perturb(dm_, nv_, U_.p, x, jf_scal_.p, jf_U_.p, active, stream_);
+    }
+    const DevFields base = df_;
+    df_.U = jf_U_.p;
+    df_.res = jf_res_.p;
+    try {
+        evaluate_residual();
+    } catch (...) {
+        df_ = base;
+        throw;
+    }
+    df_ = base;
+    const double diag = unsteady_ ? (bdf_cur_ == 2 ? 1.5 : 1.0) / cfg_.dt_physical : 0.0;
+    ProfScope ps(&prof_, CFDG_KCAT_JFNK, stream_, 1,
+                 N * 8.0 * (4.0 + (ds.n == 0 ? 0.0 : ds.n == 1 ? 1.0 : 2.0)) + double(dm_.n) * (16.0 + 4.0));
+    const int nb = launch_jf_combine(dm_, nv_, alpha_.p, diag, x, b_.p, jf_res_.p, jf_scal_.p, y, ds, partials,
+                                     active, stream_);
+    cuda_check(cudaGetLastError(), "jacobian-free product launch");
+    return nb;
 }
 
 void Solver::learn_alloc() {
@@ -1526,18 +1629,28 @@ cfdg_step_result Solver::newton_step(double cfl) {
         }
         ds_phase_ = (ds_phase_ + 1) % ds_stride_;
     }
+    const double* scale = nullptr;
+    if (last_jf_ && cfg_.jf_max_change > 0.0) {
+        ProfScope ps(&prof_, CFDG_KCAT_JFNK, stream_, 2, double(dm_.n) * (nv_ * 8.0 + 16.0 + 4.0));
+        launch_jf_step_scale(dm_, nv_, U_.p, du_.p, jf_part_.p, jf_scal_.p, cfg_.jf_max_change, stream_);
+        scale = jf_scal_.p + kJfStep;
+        cuda_check(cudaMemcpyAsync(jf_host_, scale, sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H");
+    }
     {
         ProfScope ps(&prof_, CFDG_KCAT_UPDATE, stream_, 1, ab_.state_update);
-        launch_state_update(dm_, U_.p, du_.p, nv_, stream_);
+        launch_state_update(dm_, U_.p, du_.p, nv_, scale, stream_);
     }
     if (guess_ || dataset_) {
         cuda_check(cudaMemcpyAsync(du_prev_.p, du_.p, du_.count * sizeof(double), cudaMemcpyDeviceToDevice, stream_),
                    "D2D");
         have_prev_ = true;
     }
-    residual_norms(r.l2);
+    residual_norms(r.l2);  // synchronises the stream: jf_host_ is valid after it
     r.cfl = cfl;
     r.nvars = nv_;
+    r.jacobian_free = last_jf_ ? 1 : 0;
+    r.picard_fallback = last_fallback_ ? 1 : 0;
+    r.step_scale = scale ? jf_host_[0] : 1.0;
     r.krylov_status = kr.status;
     r.krylov_iterations = kr.iterations;
     r.krylov_initial = kr.initial_residual;
@@ -1565,11 +1678,19 @@ cfdg_run_result Solver::run_steady() {
     bool have0 = false;
     const int interval = std::max(cfg_.residual_interval, 1);
     const bool robust = cfg_.convergence_monitor == 1;
+    // switched evolution relaxation: the monitor at the ramp's end
+    const bool ser = cfg_.cfl_ser_max > cfg_.cfl_max;
+    const int64_t ramp = std::max(cfg_.cfl_ramp_iterations, 1);
+    double rel_ramp = -1.0;
     for (int64_t iter = 1; iter <= cfg_.max_iterations; ++iter) {
         cfdg_step_result st;
         if (cfg_.limiter_freeze > 0 && iter >= cfg_.limiter_freeze) limiter_frozen_ = true;
+        double cfl = cfl_at(iter);
+        if (ser && rel_ramp > 0.0 && iter > ramp && out.rel > 0.0)
+            cfl = std::min(cfg_.cfl_ser_max, cfg_.cfl_max * std::max(1.0, rel_ramp / out.rel));
+        out.cfl_last = cfl;
         try {
-            st = newton_step(cfl_at(iter));
+            st = newton_step(cfl);
         } catch (const Failure& f) {
             // a non-finite state shows up in the diagonal blocks before the
             // residual norms: the reference's "blowup" exit (solver.hpp:625-629)
@@ -1580,6 +1701,8 @@ cfdg_run_result Solver::run_steady() {
         }
         out.iterations = iter;
         out.krylov_iterations_total += st.krylov_iterations;
+        out.jacobian_free_steps += st.jacobian_free;
+        out.picard_fallbacks += st.picard_fallback;
         const bool diagnose = iter == 1 || iter % interval == 0 || iter == cfg_.max_iterations;
         if (!diagnose) continue;
         bool finite = true;
@@ -1612,6 +1735,7 @@ cfdg_run_result Solver::run_steady() {
         double rel = 0.0;
         for (int k = 0; k < nm; ++k) rel = std::max(rel, mon[k] / std::max(ref_norm[k], 1.0e-300));
         out.rel = rel;
+        if (ser && rel_ramp < 0.0 && iter >= ramp) rel_ramp = rel;
         if (rel <= cfg_.residual_tolerance) {
             out.converged = 1;
             break;

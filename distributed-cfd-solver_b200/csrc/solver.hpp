@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -173,6 +174,12 @@ public:
     int64_t launches() const { return prof_->launches; }
     void set_profiler(Profiler* p) { prof_ = p ? p : &own_prof_; }
     Profiler* profiler() { return prof_; }
+    // Matrix-free Krylov operator: y = Op x with the dots `ds`, returning
+    // the partial rows written (null: the stored matrix).  The preconditioner
+    // keeps using the stored matrix; the iterations run in the host loop.
+    using Product = std::function<int(const double* x, double* y, const DotSpec& ds, double* partials,
+                                      const int* active)>;
+    void set_product(Product p) { product_ = std::move(p); }
     int check_every = 1;  // host loop: polls the Krylov state every k iterations
     bool device_loop = true;  // run the iterations as one graph launch (CFDG_KRYLOV_DEVICE_LOOP)
 
@@ -236,6 +243,7 @@ private:
     bool loop_failed_ = false;
     Profiler own_prof_;
     Profiler* prof_ = &own_prof_;
+    Product product_;
 };
 
 // The compressible finite-volume solver on one device.
@@ -306,6 +314,17 @@ private:
     bool have_prev_ = false, last_used_guess_ = false;
     void prepare_guess_inputs();
     void learn_alloc();
+    // Jacobian-free Newton-Krylov (CFDG_NEWTON_JACOBIAN_FREE): the perturbed
+    // state and its residual (SoA, cell order), reduction partials, the
+    // device scalars (kJfScalars) and a pinned host copy of the step factor
+    DevArray<double> jf_U_, jf_res_, jf_part_, jf_scal_;
+    double* jf_host_ = nullptr;
+    bool last_jf_ = false, last_fallback_ = false;
+    bool jf_now() const {
+        return cfg_.newton_operator == CFDG_NEWTON_JACOBIAN_FREE && (!muscl_ || limiter_frozen_);
+    }
+    void jf_alloc();
+    int jf_product(const double* x, double* y, const DotSpec& ds, double* partials, const int* active);
     DevMesh dm_{};
     DevFields df_{};
     SaParams sap_{};

@@ -117,7 +117,7 @@ enum {
     CFDG_KCAT_PRIMITIVES = 0, CFDG_KCAT_GRADIENT = 1, CFDG_KCAT_LIMITER = 2, CFDG_KCAT_FACE_FLUX = 3,
     CFDG_KCAT_CELL_GATHER = 4, CFDG_KCAT_JACOBIAN = 5, CFDG_KCAT_LU = 6, CFDG_KCAT_SPMV = 7, CFDG_KCAT_SGS = 8,
     CFDG_KCAT_KRYLOV = 9, CFDG_KCAT_UPDATE = 10, CFDG_KCAT_TURBULENCE = 11,
-    CFDG_KCAT_GUESS = 12, CFDG_KCAT_COUNT = 13
+    CFDG_KCAT_GUESS = 12, CFDG_KCAT_JFNK = 13, CFDG_KCAT_COUNT = 14
 };
 
 /* ------------------------------------------------------------- structures */
@@ -172,6 +172,21 @@ enum { CFDG_TIME_STEADY = 0, CFDG_TIME_UNSTEADY = 1 };
  * and with it the frozen problem, depend on every rounding before it). */
 enum { CFDG_PREFREEZE_CONFIGURED = 0, CFDG_PREFREEZE_FP64 = 1 };
 
+/* Newton operator (cfdg_config.newton_operator).  PICARD: the Krylov
+ * products use the assembled first-order matrix, as the reference's
+ * BackwardEuler does (time/implicit_euler.hpp:34-76).  JACOBIAN_FREE (not in
+ * the reference): once the limiter is frozen (from the first iteration
+ * without MUSCL) the products are the directional derivative of the full
+ * second-order residual, v -> (V/dt) v + (R(U + eps v) - R(U)) / eps, with
+ * one eps per product that moves no conserved variable by more than
+ * jf_eps of its RMS; SGS on the assembled matrix stays the preconditioner.
+ * A Jacobian-free solve that does not reduce its residual is replaced by
+ * the Picard solve of the same step, and a Jacobian-free step is relaxed
+ * so that rho and rho E (and rho nu~, against |rho nu~| + 1e-3 of its RMS)
+ * change by at most jf_max_change in any cell.  The residual, and with it
+ * the converged state, is the same; only the path to it changes. */
+enum { CFDG_NEWTON_PICARD = 0, CFDG_NEWTON_JACOBIAN_FREE = 1 };
+
 /* Solver configuration: SolverConfig + linalg::SolverParams
  * (include/cfd/solver/compressible/config.hpp:94-136, linalg/config.hpp:14-26)
  * plus the CFL ramp, precision, SGS ordering, SA and learned-guess options. */
@@ -222,6 +237,15 @@ typedef struct cfdg_config {
     int64_t max_time_steps;
     int32_t time_mode;
     int32_t bdf_order;
+    int32_t newton_operator;  /* CFDG_NEWTON_*                                */
+    int32_t jf_max_iterations; /* Krylov cap of a Jacobian-free solve          */
+    double jf_rel_tol;        /* relative tolerance of a Jacobian-free solve   */
+    double jf_eps;            /* product step: fraction of each variable's RMS */
+    double jf_max_change;     /* relaxation of Jacobian-free steps (0: off)    */
+    /* Switched evolution relaxation after the CFL ramp (run_steady):
+     * CFL = cfl_max * max(1, rel at the ramp's end / rel of the last
+     * iteration), at most cfl_ser_max; off when cfl_ser_max <= cfl_max. */
+    double cfl_ser_max;
 } cfdg_config;
 
 typedef struct cfdg_krylov_result {
@@ -238,6 +262,9 @@ typedef struct cfdg_step_result {
     int32_t guess_used;        /* 0 zero guess, 1 learned guess, 2 learned guess rejected */
     double krylov_initial, krylov_final;
     double krylov_rhs;         /* ||b||: krylov_initial / krylov_rhs < 1 when the guess helped */
+    int32_t jacobian_free;     /* 1: the update came from a Jacobian-free solve */
+    int32_t picard_fallback;   /* 1: a Jacobian-free solve failed and the Picard solve replaced it */
+    double step_scale;         /* relaxation factor applied to the update (1: none) */
 } cfdg_step_result;
 
 typedef struct cfdg_run_result {
@@ -246,6 +273,9 @@ typedef struct cfdg_run_result {
     double rel, seconds;
     int64_t krylov_iterations_total;
     double l2_first[6], l2_last[6];
+    int64_t jacobian_free_steps;      /* updates from Jacobian-free solves    */
+    int64_t picard_fallbacks;         /* Jacobian-free solves replaced by Picard */
+    double cfl_last;                  /* CFL of the last iteration            */
 } cfdg_run_result;
 
 typedef struct cfdg_unsteady_result {
