@@ -49,6 +49,7 @@ KRYLOV_DEVICE_LOOP, KRYLOV_HOST_LOOP = 0, 1
 PREFREEZE_CONFIGURED, PREFREEZE_FP64 = 0, 1
 TIME_STEADY, TIME_UNSTEADY = 0, 1
 NEWTON_PICARD, NEWTON_JACOBIAN_FREE = 0, 1
+JF_BICGSTAB, JF_GMRES = 0, 1
 STAGE_PRIMITIVES, STAGE_GRADIENT, STAGE_LIMITER, STAGE_FLUXES = range(4)
 KCAT_NAMES = ("primitives", "gradient", "limiter", "face_flux", "cell_gather", "jacobian", "lu", "spmv", "sgs",
               "krylov", "update", "turbulence", "guess", "jfnk")
@@ -96,7 +97,7 @@ class Config(C.Structure):
                 ("dt_physical", C.c_double), ("max_time_steps", C.c_int64), ("time_mode", C.c_int32),
                 ("bdf_order", C.c_int32), ("newton_operator", C.c_int32), ("jf_max_iterations", C.c_int32),
                 ("jf_rel_tol", C.c_double), ("jf_eps", C.c_double), ("jf_max_change", C.c_double),
-                ("cfl_ser_max", C.c_double)]
+                ("cfl_ser_max", C.c_double), ("jf_krylov", C.c_int32), ("jf_restart", C.c_int32)]
 
 
 class UnsteadyResult(C.Structure):
@@ -216,6 +217,10 @@ _SIGS = {
                                 C.POINTER(KrylovResult)]),
     "cfdg_bicgstab_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_int32, _dp, _dp,
                                      C.POINTER(KrylovResult)]),
+    "cfdg_gmres": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_void_p,
+                             C.c_void_p, C.POINTER(KrylovResult)]),
+    "cfdg_gmres_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32, _dp, _dp,
+                                  C.POINTER(KrylovResult)]),
 }
 
 
@@ -260,7 +265,7 @@ CONFIG_DEFAULTS = dict(
     lin_rel_tol=1.0e-1, lin_abs_tol=1.0e-15, nu_inf_ratio=3.0, max_iterations=10000,
     dt_physical=1.0e-6, max_time_steps=1, time_mode=TIME_STEADY, bdf_order=2,
     newton_operator=NEWTON_PICARD, jf_max_iterations=60, jf_rel_tol=1.0e-2, jf_eps=1.0e-7, jf_max_change=0.2,
-    cfl_ser_max=0.0)
+    cfl_ser_max=0.0, jf_krylov=JF_GMRES, jf_restart=30)
 
 
 def default_config(**overrides) -> Config:
@@ -708,6 +713,14 @@ class Bsr:
         x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
         r = KrylovResult()
         check(lib().cfdg_bicgstab_host(self._h, precond, rel_tol, abs_tol, max_it, _dptr(x), _dptr(b), C.byref(r)))
+        return x, r
+
+    def gmres(self, b, x0=None, precond=PC_SGS, rel_tol=1e-8, abs_tol=1e-30, max_it=500, restart=30):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        r = KrylovResult()
+        check(lib().cfdg_gmres_host(self._h, precond, rel_tol, abs_tol, max_it, restart, _dptr(x), _dptr(b),
+                                    C.byref(r)))
         return x, r
 
 

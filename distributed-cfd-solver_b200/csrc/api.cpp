@@ -158,6 +158,8 @@ void cfdg_config_default(cfdg_config* c) {
     c->jf_eps = 1.0e-7;
     c->jf_max_change = 0.2;
     c->cfl_ser_max = 0.0;
+    c->jf_krylov = CFDG_JF_GMRES;
+    c->jf_restart = 30;
 }
 
 // ------------------------------------------------------------------ meshes
@@ -456,6 +458,29 @@ int cfdg_bicgstab_host(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_
         x.make(N, a->stream, x_h);
         b.make(N, a->stream, b_h);
         const cfdg_krylov_result r = a->impl->bicgstab(precond, rel_tol, abs_tol, max_it, x.d, b.d);
+        x.get(x_h, N, a->stream);
+        if (out_h) *out_h = r;
+    });
+}
+
+int cfdg_gmres(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it, int32_t restart,
+               double* x_d, const double* b_d, cfdg_krylov_result* out_h) {
+    if (!x_d || !b_d) return CFDG_ERR_INVALID;
+    CFDG_BSR_CALL(a, {
+        const cfdg_krylov_result r = a->impl->gmres(precond, rel_tol, abs_tol, max_it, restart, x_d, b_d);
+        if (out_h) *out_h = r;
+    });
+}
+
+int cfdg_gmres_host(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it, int32_t restart,
+                    double* x_h, const double* b_h, cfdg_krylov_result* out_h) {
+    if (!x_h || !b_h) return CFDG_ERR_INVALID;
+    CFDG_BSR_CALL(a, {
+        const std::size_t N = static_cast<std::size_t>(a->impl->n()) * a->impl->bs();
+        HostVec x, b;
+        x.make(N, a->stream, x_h);
+        b.make(N, a->stream, b_h);
+        const cfdg_krylov_result r = a->impl->gmres(precond, rel_tol, abs_tol, max_it, restart, x.d, b.d);
         x.get(x_h, N, a->stream);
         if (out_h) *out_h = r;
     });

@@ -97,6 +97,18 @@ void launch_jf_perturb(const DevMesh& m, int nv, const double* U, const double* 
 void launch_jf_step_scale(const DevMesh& m, int nv, const double* U, const double* du, double* partials, double* scal,
                           double max_change, cudaStream_t s);
 
+// ------------------------------------------------------ restarted GMRES
+// Basis V: vectors k at V + k*ld.  h[k0 + k] = V_{k0+k} . w for k < kn
+// (partials: gm_partial_blocks(len) * gm_chunk() doubles); w -= sum h_k V_k
+// (subtract) or w = sum h_k V_k; y = a x (+ y).
+int gm_partial_blocks(int64_t len);
+int gm_chunk();
+void launch_gm_dots(int64_t len, const double* V, int64_t ld, int k0, int kn, const double* w, double* partials,
+                    double* h, cudaStream_t s);
+void launch_gm_update(int64_t len, const double* V, int64_t ld, int kn, const double* h, double* w, bool subtract,
+                      cudaStream_t s);
+void launch_gm_axpy(int64_t len, double a, const double* x, double* y, bool accumulate, cudaStream_t s);
+
 // ------------------------------------------------------------ linear algebra
 struct BsrView {
     int32_t n, bs;

@@ -265,6 +265,7 @@ BsrSystem::BsrSystem(int device, int32_t n, int32_t bs, const int32_t* row_ptr, 
 BsrSystem::~BsrSystem() {
     release_device_loop();
     if (ks_host_) cudaFreeHost(ks_host_);
+    if (gm_h_host_) cudaFreeHost(gm_h_host_);
 }
 
 void BsrSystem::set_precision(int precision) {
@@ -778,6 +779,210 @@ cfdg_krylov_result BsrSystem::bicgstab(int precond, double rel_tol, double abs_t
     return res;
 }
 
+void BsrSystem::gm_alloc(int restart) {
+    if (gm_restart_ == restart) return;
+    const std::size_t N = static_cast<std::size_t>(n_) * bs_;
+    gm_V_.release();
+    alloc_or_throw(gm_V_, N * (restart + 1), "GMRES basis");
+    alloc_or_throw(gm_z_, N, "GMRES vector");
+    alloc_or_throw(gm_part_, static_cast<std::size_t>(gm_partial_blocks(int64_t(N))) * gm_chunk() + 8, "GMRES partials");
+    alloc_or_throw(gm_h_, 3 * static_cast<std::size_t>(restart + 1) + 8, "GMRES coefficients");
+    cuda_check(cudaMemsetAsync(gm_h_.p, 0, gm_h_.count * sizeof(double), stream_), "memset");
+    if (gm_h_host_) cudaFreeHost(gm_h_host_);
+    gm_h_host_ = nullptr;
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&gm_h_host_), sizeof(double) * (3 * (restart + 1) + 8)),
+               "cudaMallocHost");
+    gm_restart_ = restart;
+}
+
+// GMRES(m) with right preconditioning (Saad, Iterative Methods for Sparse
+// Linear Systems, 2nd ed., Alg. 9.5): Arnoldi on A M^-1 by classical
+// Gram-Schmidt with one reorthogonalisation pass, Givens rotations of the
+// Hessenberg column on the host (one coefficient read per iteration), the
+// update x += M^-1 V y at the end of each cycle and the true residual at
+// each restart.  The residual estimate |g_{j+1}| decreases monotonically.
+cfdg_krylov_result BsrSystem::gmres(int precond, double rel_tol, double abs_tol, int max_it, int restart, double* x,
+                                    const double* b, bool guess) {
+    if (precond == CFDG_PC_SGS && !lu_ready_) throw Failure{CFDG_ERR_INVALID, "SGS preconditioner not set up"};
+    if (restart < 1 || restart > 200) throw Failure{CFDG_ERR_INVALID, "GMRES restart must be in [1, 200]"};
+    gm_alloc(restart);
+    const int64_t N = int64_t(n_) * bs_;
+    const BsrView A = view();
+    const bool mixed = precision_ == CFDG_PREC_MIXED;
+    const int m = restart;
+    double* V = gm_V_.p;
+    double* hd = gm_h_.p;        // [0, m+1) first projection, [m+1, 2m+2) second, [2m+2] |w|^2
+    double* hh = gm_h_host_;
+    DotSpec none{};
+    none.n = 0;
+    auto vec = [&](int k) { return V + int64_t(k) * N; };
+    auto apply_A = [&](const double* xin, double* yout) {
+        if (product_) {
+            product_(xin, yout, none, nullptr, nullptr);
+            return;
+        }
+        ProfScope ps(prof_, CFDG_KCAT_SPMV, stream_, 1, spmv_bytes(0, false));
+        if (mixed) launch_spmv_ex<float>(A, vals32_.p, xin, yout, 1.0, 0.0, none, nullptr, nullptr, stream_);
+        else launch_spmv_ex<double>(A, vals64_.p, xin, yout, 1.0, 0.0, none, nullptr, nullptr, stream_);
+    };
+    auto precond_apply = [&](const double* r, double* z) {
+        if (precond == CFDG_PC_SGS) {
+            sgs_apply(r, z, nullptr);
+        } else {
+            ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 1, 16.0 * N);
+            cuda_check(cudaMemcpyAsync(z, r, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream_), "D2D");
+        }
+    };
+    const int chunk = gm_chunk();
+    auto dots = [&](int kn, const double* w, double* h) {
+        ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 2 * ((kn + chunk - 1) / chunk),
+                     8.0 * N * (kn + (kn + chunk - 1) / chunk));
+        launch_gm_dots(N, V, N, 0, kn, w, gm_part_.p, h, stream_);
+    };
+    auto norm2 = [&](const double* w, double* h) {
+        ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 2, 8.0 * N);
+        launch_gm_dots(N, w, 0, 0, 1, w, gm_part_.p, h, stream_);
+    };
+    auto read_h = [&](int count) {
+        cuda_check(cudaMemcpyAsync(hh, hd, sizeof(double) * count, cudaMemcpyDeviceToHost, stream_), "D2H");
+        cuda_check(cudaStreamSynchronize(stream_), "gmres sync");
+    };
+    auto axpy = [&](double a, const double* xin, double* y, bool acc) {
+        ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 1, 8.0 * N * (acc ? 3.0 : 2.0));
+        launch_gm_axpy(N, a, xin, y, acc, stream_);
+    };
+    // r0 = b - A x in V_0; ||b||
+    norm2(b, hd + 2 * m + 2);
+    read_h(2 * m + 3);
+    const double bnorm = std::sqrt(hh[2 * m + 2]);
+    double beta = bnorm;
+    int guess_state = 0;
+    // x holds x0; with the matrix-free product and no guess the caller has
+    // zeroed it, and r0 = b needs no residual evaluation
+    bool zero_start = product_ && !guess;
+    if (!zero_start) {
+        apply_A(x, vec(0));
+        axpy(-1.0, vec(0), vec(0), false);
+        axpy(1.0, b, vec(0), true);
+        norm2(vec(0), hd + 2 * m + 2);
+        read_h(2 * m + 3);
+        beta = std::sqrt(hh[2 * m + 2]);
+        if (guess) {
+            guess_state = 1;
+            if (!(beta < bnorm)) {  // the guess does not beat x = 0
+                guess_state = 2;
+                beta = bnorm;
+                zero_start = true;
+            }
+        }
+    }
+    if (zero_start) {
+        cuda_check(cudaMemsetAsync(x, 0, sizeof(double) * N, stream_), "memset");
+        cuda_check(cudaMemcpyAsync(vec(0), b, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream_), "D2D");
+    }
+    const double tol = std::max(abs_tol, rel_tol * (bnorm > 0.0 ? bnorm : 1.0));
+    cfdg_krylov_result res{};
+    res.initial_residual = beta;
+    res.final_residual = beta;
+    int its = 0;
+    int state = std::isfinite(beta) ? (beta <= tol ? KS_CONVERGED : KS_RUNNING) : KS_DIVERGED;
+    std::vector<double> R(static_cast<std::size_t>(m) * m), g(m + 1), cs(m), sn(m), y(m);
+    while (state == KS_RUNNING) {
+        axpy(1.0 / beta, vec(0), vec(0), false);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int k = 0;
+        double resid = beta;
+        for (int j = 0; j < m && its < max_it; ++j) {
+            double* w = vec(j + 1);
+            precond_apply(vec(j), gm_z_.p);
+            apply_A(gm_z_.p, w);
+            dots(j + 1, w, hd);
+            {
+                ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 1, 8.0 * N * (j + 3));
+                launch_gm_update(N, V, N, j + 1, hd, w, true, stream_);
+            }
+            dots(j + 1, w, hd + m + 1);
+            {
+                ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 1, 8.0 * N * (j + 3));
+                launch_gm_update(N, V, N, j + 1, hd + m + 1, w, true, stream_);
+            }
+            norm2(w, hd + 2 * m + 2);
+            read_h(2 * m + 3);
+            ++its;
+            double col[201];
+            for (int i = 0; i <= j; ++i) col[i] = hh[i] + hh[m + 1 + i];
+            const double hn = std::sqrt(std::max(hh[2 * m + 2], 0.0));
+            col[j + 1] = hn;
+            for (int i = 0; i < j; ++i) {  // previous rotations
+                const double t = cs[i] * col[i] + sn[i] * col[i + 1];
+                col[i + 1] = -sn[i] * col[i] + cs[i] * col[i + 1];
+                col[i] = t;
+            }
+            const double rr = std::hypot(col[j], col[j + 1]);
+            if (!(rr > 0.0) || !std::isfinite(rr)) {
+                state = KS_DIVERGED;
+                break;
+            }
+            cs[j] = col[j] / rr;
+            sn[j] = col[j + 1] / rr;
+            col[j] = rr;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            for (int i = 0; i <= j; ++i) R[static_cast<std::size_t>(i) * m + j] = col[i];
+            k = j + 1;
+            resid = std::fabs(g[j + 1]);
+            if (resid <= tol || hn == 0.0) {
+                state = KS_CONVERGED;
+                break;
+            }
+            axpy(1.0 / hn, w, w, false);
+        }
+        if (k > 0) {
+            // y = R^-1 g, x += M^-1 (V y)
+            for (int i = k - 1; i >= 0; --i) {
+                double s = g[i];
+                for (int l = i + 1; l < k; ++l) s -= R[static_cast<std::size_t>(i) * m + l] * y[l];
+                y[i] = s / R[static_cast<std::size_t>(i) * m + i];
+            }
+            cuda_check(cudaMemcpyAsync(hd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stream_), "H2D");
+            {
+                ProfScope ps(prof_, CFDG_KCAT_KRYLOV, stream_, 1, 8.0 * N * (k + 1));
+                launch_gm_update(N, V, N, k, hd, gm_z_.p, false, stream_);
+            }
+            precond_apply(gm_z_.p, vec(k));
+            axpy(1.0, vec(k), x, true);
+            cuda_check(cudaStreamSynchronize(stream_), "gmres sync");  // y on the host stays alive until here
+        }
+        res.final_residual = resid;
+        if (state != KS_RUNNING) break;
+        if (its >= max_it) {
+            state = KS_MAXIT;
+            break;
+        }
+        // restart from the true residual
+        apply_A(x, vec(0));
+        axpy(-1.0, vec(0), vec(0), false);
+        axpy(1.0, b, vec(0), true);
+        norm2(vec(0), hd + 2 * m + 2);
+        read_h(2 * m + 3);
+        beta = std::sqrt(hh[2 * m + 2]);
+        res.final_residual = beta;
+        if (!std::isfinite(beta)) state = KS_DIVERGED;
+        else if (beta <= tol) state = KS_CONVERGED;
+    }
+    cuda_check(cudaGetLastError(), "gmres launch");
+    last_guess_ = guess ? guess_state : 0;
+    last_bnorm_ = bnorm;
+    switch (state) {
+        case KS_CONVERGED: res.status = CFDG_KRYLOV_CONVERGED; break;
+        case KS_DIVERGED: res.status = CFDG_KRYLOV_DIVERGED; break;
+        default: res.status = CFDG_KRYLOV_MAX_ITERATIONS; break;
+    }
+    res.iterations = its;
+    return res;
+}
+
 // ================================================================= Solver
 Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, const cfdg_bc_desc* bcs, int n_bcs)
     : device_(device), cfg_(cfg) {
@@ -806,6 +1011,10 @@ Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, c
         (!(cfg.jf_eps > 0.0) || !(cfg.jf_rel_tol > 0.0) || cfg.jf_max_iterations < 1 || !(cfg.jf_max_change >= 0.0)))
         throw Failure{CFDG_ERR_INVALID,
                       "Jacobian-free Newton needs jf_eps > 0, jf_rel_tol > 0, jf_max_iterations >= 1, jf_max_change >= 0"};
+    if (cfg.newton_operator == CFDG_NEWTON_JACOBIAN_FREE &&
+        ((cfg.jf_krylov != CFDG_JF_BICGSTAB && cfg.jf_krylov != CFDG_JF_GMRES) ||
+         (cfg.jf_krylov == CFDG_JF_GMRES && (cfg.jf_restart < 1 || cfg.jf_restart > 200))))
+        throw Failure{CFDG_ERR_INVALID, "jf_krylov must be CFDG_JF_BICGSTAB or CFDG_JF_GMRES with jf_restart in [1, 200]"};
     unsteady_ = cfg.time_mode == CFDG_TIME_UNSTEADY;
     if (unsteady_ && (cfg.bdf_order < 1 || cfg.bdf_order > 2 || !(cfg.dt_physical > 0.0) || cfg.max_time_steps < 0))
         throw Failure{CFDG_ERR_INVALID, "unsteady mode needs bdf_order 1 or 2, dt_physical > 0, max_time_steps >= 0"};
@@ -1483,8 +1692,12 @@ cfdg_krylov_result Solver::linear_solve() {
     });
     cfdg_krylov_result kr{};
     try {
-        kr = sys_->bicgstab(cfg_.precond, cfg_.jf_rel_tol, cfg_.lin_abs_tol, cfg_.jf_max_iterations, du_.p, b_.p,
-                            use_guess);
+        if (cfg_.jf_krylov == CFDG_JF_GMRES)
+            kr = sys_->gmres(cfg_.precond, cfg_.jf_rel_tol, cfg_.lin_abs_tol, cfg_.jf_max_iterations, cfg_.jf_restart,
+                             du_.p, b_.p, use_guess);
+        else
+            kr = sys_->bicgstab(cfg_.precond, cfg_.jf_rel_tol, cfg_.lin_abs_tol, cfg_.jf_max_iterations, du_.p, b_.p,
+                                use_guess);
     } catch (...) {
         sys_->set_product(nullptr);
         throw;

@@ -167,6 +167,11 @@ public:
     // ||b - A x|| >= ||b||; last_guess() tells 1 accepted, 2 rejected.
     cfdg_krylov_result bicgstab(int precond, double rel_tol, double abs_tol, int max_it, double* x, const double* b,
                                 bool guess = false);
+    // Restarted GMRES(restart), right-preconditioned, on the same operator
+    // (the stored matrix or the matrix-free product); same conventions as
+    // bicgstab.  The basis is allocated on first use.
+    cfdg_krylov_result gmres(int precond, double rel_tol, double abs_tol, int max_it, int restart, double* x,
+                             const double* b, bool guess = false);
     int last_guess() const { return last_guess_; }
     double last_bnorm() const { return last_bnorm_; }
     int groups_fwd() const { return static_cast<int>(fwd_off_.size()) - 1; }
@@ -244,6 +249,12 @@ private:
     Profiler own_prof_;
     Profiler* prof_ = &own_prof_;
     Product product_;
+    // GMRES workspace: basis (restart + 1 vectors), a vector, partials,
+    // device and pinned host coefficients (3 x (restart + 1) + 8)
+    DevArray<double> gm_V_, gm_z_, gm_part_, gm_h_;
+    double* gm_h_host_ = nullptr;
+    int gm_restart_ = 0;
+    void gm_alloc(int restart);
 };
 
 // The compressible finite-volume solver on one device.

@@ -187,6 +187,11 @@ enum { CFDG_PREFREEZE_CONFIGURED = 0, CFDG_PREFREEZE_FP64 = 1 };
  * the converged state, is the same; only the path to it changes. */
 enum { CFDG_NEWTON_PICARD = 0, CFDG_NEWTON_JACOBIAN_FREE = 1 };
 
+/* Krylov method of the Jacobian-free solves (cfdg_config.jf_krylov):
+ * BiCGSTAB as for the Picard matrix, or restarted GMRES(jf_restart) with
+ * right preconditioning, whose residual never grows. */
+enum { CFDG_JF_BICGSTAB = 0, CFDG_JF_GMRES = 1 };
+
 /* Solver configuration: SolverConfig + linalg::SolverParams
  * (include/cfd/solver/compressible/config.hpp:94-136, linalg/config.hpp:14-26)
  * plus the CFL ramp, precision, SGS ordering, SA and learned-guess options. */
@@ -246,6 +251,8 @@ typedef struct cfdg_config {
      * CFL = cfl_max * max(1, rel at the ramp's end / rel of the last
      * iteration), at most cfl_ser_max; off when cfl_ser_max <= cfl_max. */
     double cfl_ser_max;
+    int32_t jf_krylov;        /* CFDG_JF_*                                    */
+    int32_t jf_restart;       /* GMRES restart length, 1..200                 */
 } cfdg_config;
 
 typedef struct cfdg_krylov_result {
@@ -462,6 +469,13 @@ CFDG_API int cfdg_bicgstab(cfdg_bsr* a, int32_t precond, double rel_tol, double 
                   double* x_d, const double* b_d, cfdg_krylov_result* out_h);
 CFDG_API int cfdg_bicgstab_host(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it,
                        double* x_h, const double* b_h, cfdg_krylov_result* out_h);
+/* Restarted GMRES(restart) with right preconditioning (not in the
+ * reference; the Krylov method of the Jacobian-free solves, CFDG_JF_GMRES);
+ * same arguments and conventions as cfdg_bicgstab, restart in [1, 200]. */
+CFDG_API int cfdg_gmres(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it, int32_t restart,
+               double* x_d, const double* b_d, cfdg_krylov_result* out_h);
+CFDG_API int cfdg_gmres_host(cfdg_bsr* a, int32_t precond, double rel_tol, double abs_tol, int32_t max_it,
+                    int32_t restart, double* x_h, const double* b_h, cfdg_krylov_result* out_h);
 
 /* ------------------------------------------------ learned initial guess
  * Not in the reference (its BiCGSTAB starts from the zero vector,

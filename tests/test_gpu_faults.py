@@ -34,6 +34,22 @@ def test_zero_rhs_and_max_iterations(cb):
     assert info.status == cb.KRYLOV_MAX_ITERATIONS and info.iterations == 0
 
 
+def test_gmres_edge_cases(cb):
+    # identity: one iteration, exact; zero right-hand side: no iteration;
+    # max_it = 0: no iteration, max-iterations status
+    A = _eye_bsr(cb, scale=2.0)
+    b = np.arange(1.0, 61.0)
+    x, info = A.gmres(b, precond=cb.PC_NONE, rel_tol=1e-12)
+    assert info.status == cb.KRYLOV_CONVERGED and info.iterations == 1
+    assert np.allclose(x, b / 2.0, rtol=1e-14, atol=0.0)
+    x, info = A.gmres(np.zeros(60), precond=cb.PC_NONE)
+    assert info.status == cb.KRYLOV_CONVERGED and info.iterations == 0
+    x, info = A.gmres(np.ones(60), precond=cb.PC_NONE, max_it=0)
+    assert info.status == cb.KRYLOV_MAX_ITERATIONS and info.iterations == 0
+    with pytest.raises(cb.CfdgError):
+        A.gmres(np.ones(60), precond=cb.PC_NONE, restart=0)
+
+
 def test_singular_diagonal_block_reported(cb):
     n, bs = 8, 5
     rp = np.arange(n + 1, dtype=np.int32)

@@ -138,6 +138,42 @@ def test_spmv_sgs_level_bicgstab(cb, refh, name):
     assert rel_err(sol_n, sol_nr) < 1e-6
 
 
+@pytest.mark.parametrize("name", ["ramp_muscl", "bump_tets"])
+def test_gmres_matches_reference_solution(cb, refh, name):
+    """Restarted GMRES (the Jacobian-free solves' Krylov method) on the
+    reference's matrices: the solution of the reference's BiCGSTAB to the
+    tolerance, with SGS (level and multicolour) and without a
+    preconditioner, with and without restarts; x0 != 0 is honoured."""
+    row_ptr, cols, vals = _matrix_from_ref(cb, refh, name)
+    n = len(row_ptr) - 1
+    rng = np.random.default_rng(4)
+    b = rng.standard_normal(n * 5)
+    A = cb.Bsr(row_ptr, cols, 5)
+    A.set_values(vals)
+    sol_ref, info_ref = refh.bicgstab(row_ptr, cols, vals, 5, b, precond=1, rel_tol=1e-12, max_it=400)
+    assert info_ref["status"] == 0
+    for ordering, restart in [(cb.SGS_LEVEL, 30), (cb.SGS_COLOR, 30), (cb.SGS_COLOR, 5)]:
+        A.sgs_setup(ordering, 1)
+        sol, info = A.gmres(b, precond=cb.PC_SGS, rel_tol=1e-10, max_it=600, restart=restart)
+        assert info.status == cb.KRYLOV_CONVERGED, (ordering, restart, info.iterations)
+        assert info.final_residual <= 1e-10 * np.linalg.norm(b) * (1 + 1e-9)
+        assert rel_err(sol, sol_ref) < 1e-7, (ordering, restart)
+        # the true residual agrees with the estimate
+        r = b - A.spmv(sol, np.zeros_like(b), 1.0, 0.0)
+        assert np.linalg.norm(r) < 1e-8 * np.linalg.norm(b)
+    sol_n, info_n = A.gmres(b, precond=cb.PC_NONE, rel_tol=1e-10, max_it=3000, restart=60)
+    assert info_n.status == cb.KRYLOV_CONVERGED
+    assert rel_err(sol_n, sol_ref) < 1e-6
+    # a starting vector near the solution needs fewer iterations
+    A.sgs_setup(cb.SGS_COLOR, 1)
+    _, info_0 = A.gmres(b, precond=cb.PC_SGS, rel_tol=1e-10, max_it=600)
+    x0 = sol_ref + 1e-6 * rng.standard_normal(n * 5) * np.abs(sol_ref).max()
+    sol_g, info_g = A.gmres(b, x0=x0, precond=cb.PC_SGS, rel_tol=1e-10, max_it=600)
+    assert info_g.status == cb.KRYLOV_CONVERGED and info_g.initial_residual < info_0.initial_residual
+    assert info_g.iterations < info_0.iterations
+    assert rel_err(sol_g, sol_ref) < 1e-7
+
+
 @pytest.mark.parametrize("name", ["ramp_muscl", "plate_viscous", "bump_tets"])
 def test_newton_steps_match_reference(cb, refh, name):
     case, mesh, U0, gpu, ref = _setup(cb, refh, name, level=True)
