@@ -97,7 +97,8 @@ class Config(C.Structure):
                 ("dt_physical", C.c_double), ("max_time_steps", C.c_int64), ("time_mode", C.c_int32),
                 ("bdf_order", C.c_int32), ("newton_operator", C.c_int32), ("jf_max_iterations", C.c_int32),
                 ("jf_rel_tol", C.c_double), ("jf_eps", C.c_double), ("jf_max_change", C.c_double),
-                ("cfl_ser_max", C.c_double), ("jf_krylov", C.c_int32), ("jf_restart", C.c_int32)]
+                ("cfl_ser_max", C.c_double), ("jf_krylov", C.c_int32), ("jf_restart", C.c_int32),
+                ("jf_accept", C.c_double)]
 
 
 class UnsteadyResult(C.Structure):
@@ -265,7 +266,7 @@ CONFIG_DEFAULTS = dict(
     lin_rel_tol=1.0e-1, lin_abs_tol=1.0e-15, nu_inf_ratio=3.0, max_iterations=10000,
     dt_physical=1.0e-6, max_time_steps=1, time_mode=TIME_STEADY, bdf_order=2,
     newton_operator=NEWTON_PICARD, jf_max_iterations=60, jf_rel_tol=1.0e-2, jf_eps=1.0e-7, jf_max_change=0.2,
-    cfl_ser_max=0.0, jf_krylov=JF_GMRES, jf_restart=30)
+    cfl_ser_max=0.0, jf_krylov=JF_GMRES, jf_restart=30, jf_accept=0.5)
 
 
 def default_config(**overrides) -> Config:

@@ -160,6 +160,7 @@ void cfdg_config_default(cfdg_config* c) {
     c->cfl_ser_max = 0.0;
     c->jf_krylov = CFDG_JF_GMRES;
     c->jf_restart = 30;
+    c->jf_accept = 0.5;
 }
 
 // ------------------------------------------------------------------ meshes

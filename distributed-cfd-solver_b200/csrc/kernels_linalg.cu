@@ -10,6 +10,8 @@
 //   BiCGSTAB::solve       src/linalg/bicgstab.cpp:42-201
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "kernels.hpp"
 #include "krylov.hpp"
 
@@ -51,19 +53,21 @@ __device__ __forceinline__ void load_block_row(const MT* __restrict__ a, double 
 // read-only path: the neighbour entries a sweep or product reads are not
 // written during the launch (rows of one colour or level are never
 // neighbours).  6-entry blocks are 16-byte aligned and load as pairs.
-template <int BS>
+// COHERENT: through L2 only (ld.global.cg), for entries other SMs wrote
+// earlier in the same launch (the cooperative level sweep).
+template <int BS, bool COHERENT = false>
 __device__ __forceinline__ void load_vec(const double* __restrict__ x, double (&out)[BS]) {
     if constexpr (BS == 6 || BS == 4) {
         const double2* p = reinterpret_cast<const double2*>(x);
 #pragma unroll
         for (int h = 0; h < BS / 2; ++h) {
-            const double2 v = __ldg(p + h);
+            const double2 v = COHERENT ? __ldcg(p + h) : __ldg(p + h);
             out[2 * h] = v.x;
             out[2 * h + 1] = v.y;
         }
     } else {
 #pragma unroll
-        for (int j = 0; j < BS; ++j) out[j] = __ldg(x + j);
+        for (int j = 0; j < BS; ++j) out[j] = COHERENT ? __ldcg(x + j) : __ldg(x + j);
     }
 }
 
@@ -73,7 +77,7 @@ __device__ __forceinline__ void load_vec(const double* __restrict__ x, double (&
 // neighbour's x block load as 16-byte pairs for 6x6 blocks (measured on the
 // SA plate: SGS 0.73 -> 0.80 of the copy bandwidth); other block sizes keep
 // scalar loads, which measured faster for 5x5 (FP32 tet bump).
-template <typename MT, int BS, bool SUB>
+template <typename MT, int BS, bool SUB, bool COHERENT = false>
 __device__ __forceinline__ double block_row_dot(const BsrView& A, const MT* __restrict__ vals, const double* x,
                                                 int ii, int32_t k0, int32_t k1, double acc) {
     for (int32_t k = k0; k < k1; ++k) {
@@ -81,14 +85,14 @@ __device__ __forceinline__ double block_row_dot(const BsrView& A, const MT* __re
         if constexpr (BS == 6) {
             double a[BS], xb[BS];
             load_block_row<MT, BS>(vals + int64_t(k) * (BS * BS) + ii * BS, a);
-            load_vec<BS>(x + int64_t(__ldg(A.cols + k)) * BS, xb);
+            load_vec<BS, COHERENT>(x + int64_t(__ldg(A.cols + k)) * BS, xb);
 #pragma unroll
             for (int jj = 0; jj < BS; ++jj) t += a[jj] * xb[jj];
         } else {
             const MT* a = vals + int64_t(k) * (BS * BS) + ii * BS;
             const double* xb = x + int64_t(A.cols[k]) * BS;
 #pragma unroll
-            for (int jj = 0; jj < BS; ++jj) t += ld(a + jj) * xb[jj];
+            for (int jj = 0; jj < BS; ++jj) t += ld(a + jj) * (COHERENT ? __ldcg(xb + jj) : xb[jj]);
         }
         acc = SUB ? acc - t : acc + t;
     }
@@ -384,6 +388,69 @@ __global__ void __launch_bounds__(256, (INV && BS <= 5) ? 8 : 6) k_sgs_rows(BsrV
         // MODE 3: b solved D x = -sum_upper A z, so z_i = y_i + x
         if (MODE == 3) out = z[int64_t(i) * BS + ii] + out;
         z[int64_t(i) * BS + ii] = out;
+    }
+}
+
+// The level-scheduled sweep (the reference's sequential order) in one
+// cooperative launch: the resident grid walks the forward levels, then the
+// backward levels, each level's rows by lane groups exactly as k_sgs_rows
+// MODE 0 with the pivoted LU, and a grid-wide barrier separates the levels
+// instead of a kernel boundary (about 1.2-1.6 us against a launch per level).
+// z entries written in one level are read by later levels on other SMs, so
+// z is read through L2 (ld.global.cg), never from a stale L1 line.  Every
+// loop is bounded by the level and row counts, and the cooperative launch
+// makes every block resident, so every barrier is reached by all blocks.
+template <typename MT, int BS>
+__global__ void __launch_bounds__(256) k_sgs_level_coop(BsrView A, const MT* __restrict__ vals,
+                                                        const MT* __restrict__ lu, const int8_t* __restrict__ piv,
+                                                        const int32_t* __restrict__ fwd_rows,
+                                                        const int32_t* __restrict__ fwd_off, int n_fwd,
+                                                        const int32_t* __restrict__ bwd_rows,
+                                                        const int32_t* __restrict__ bwd_off, int n_bwd,
+                                                        const double* __restrict__ r, double* z,
+                                                        const int* __restrict__ active) {
+    if (active && *active != 0) return;  // the same value for every block: all return before the first barrier
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    constexpr int GPW = 32 / BS;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const int grp = lane / BS, ii = lane - grp * BS;
+    const int base_lane = (grp < GPW ? grp : 0) * BS;
+    for (int pass = 0; pass < 2; ++pass) {
+        const int32_t* rows = pass ? bwd_rows : fwd_rows;
+        const int32_t* off = pass ? bwd_off : fwd_off;
+        const int ng = pass ? n_bwd : n_fwd;
+        for (int g = 0; g < ng; ++g) {
+            const int32_t o0 = off[g];
+            const int64_t nr = off[g + 1] - o0;
+            for (int64_t first = warp * GPW; first < nr; first += nwarps * GPW) {  // warp-uniform
+                const int64_t slot = first + grp;
+                const bool act = (grp < GPW) && (slot < nr);
+                int32_t i = 0;
+                double s = 0.0;
+                if (act) {
+                    i = rows[o0 + slot];
+                    s = r[int64_t(i) * BS + ii];
+                    const int32_t d = A.diag[i];
+                    s = block_row_dot<MT, BS, true, true>(A, vals, z, ii, A.row_ptr[i], d, s);
+                    s = block_row_dot<MT, BS, true, true>(A, vals, z, ii, d + 1, A.row_ptr[i + 1], s);
+                }
+                double b[BS];
+#pragma unroll
+                for (int j = 0; j < BS; ++j) b[j] = __shfl_sync(0xffffffffu, s, base_lane + j);
+                if (act) {
+                    lu_solve<MT, BS>(lu + int64_t(i) * (BS * BS), piv + int64_t(i) * BS, b);
+                    double out = b[0];
+#pragma unroll
+                    for (int j = 1; j < BS; ++j)
+                        if (j == ii) out = b[j];
+                    z[int64_t(i) * BS + ii] = out;
+                }
+            }
+            grid.sync();
+        }
     }
 }
 
@@ -769,6 +836,39 @@ void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const in
 #undef CFDG_SGS_M
 }
 
+template <typename MT, int BS>
+static int level_coop_grid() {
+    static int grid = -1;  // resident 256-thread blocks on every SM, once per process and instantiation
+    if (grid < 0) {
+        int dev = 0, sms = 0, per_sm = 0, coop = 0;
+        grid = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sgs_level_coop<MT, BS>, 256, 0) == cudaSuccess)
+            grid = sms * std::min(per_sm, 4);
+        cudaGetLastError();
+    }
+    return grid;
+}
+
+template <typename MT>
+bool launch_sgs_level_coop(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* fwd_rows,
+                           const int32_t* fwd_off, int n_fwd, const int32_t* bwd_rows, const int32_t* bwd_off,
+                           int n_bwd, const double* r, double* z, const int* active, cudaStream_t s) {
+    void* args[] = {const_cast<BsrView*>(&A), &vals, &lu, &piv, &fwd_rows, &fwd_off, &n_fwd, &bwd_rows, &bwd_off,
+                    &n_bwd, &r, &z, &active};
+    int grid = 0;
+    void* fn = nullptr;
+    switch (A.bs) {
+        case 5: grid = level_coop_grid<MT, 5>(); fn = reinterpret_cast<void*>(k_sgs_level_coop<MT, 5>); break;
+        case 6: grid = level_coop_grid<MT, 6>(); fn = reinterpret_cast<void*>(k_sgs_level_coop<MT, 6>); break;
+        default: return false;
+    }
+    if (grid <= 0) return false;
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256), args, 0, s) == cudaSuccess;
+}
+
 int dot_blocks(int64_t len) { return static_cast<int>(vec_grid(len)); }
 
 void launch_krylov_init(int64_t len, const double* b, const double* v, double* r, double* r0, double* p,
@@ -827,6 +927,12 @@ template void launch_sgs_last_spmv<float>(const BsrView&, const float*, const fl
                                           const DotSpec&, double*, const int*, cudaStream_t);
 template void launch_lu_setup<double>(const BsrView&, const double*, double*, int8_t*, int*, bool, cudaStream_t);
 template void launch_lu_setup<float>(const BsrView&, const float*, float*, int8_t*, int*, bool, cudaStream_t);
+template bool launch_sgs_level_coop<double>(const BsrView&, const double*, const double*, const int8_t*,
+                                            const int32_t*, const int32_t*, int, const int32_t*, const int32_t*, int,
+                                            const double*, double*, const int*, cudaStream_t);
+template bool launch_sgs_level_coop<float>(const BsrView&, const float*, const float*, const int8_t*, const int32_t*,
+                                           const int32_t*, int, const int32_t*, const int32_t*, int, const double*,
+                                           double*, const int*, cudaStream_t);
 template void launch_sgs_rows_ex<double>(const BsrView&, const double*, const double*, const int8_t*, const int32_t*,
                                          int32_t, int32_t, const double*, double*, int, bool, const int*,
                                          cudaStream_t);

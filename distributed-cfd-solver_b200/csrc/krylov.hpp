@@ -55,6 +55,14 @@ template <typename MT>
 void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* rows,
                         int32_t row0, int32_t n_rows, const double* r, double* z, int mode, bool inverse,
                         const int* active, cudaStream_t s);
+// The whole level-scheduled symmetric sweep (forward levels, then backward
+// levels; z zeroed by the caller) as one cooperative launch with a grid
+// barrier per level; false when the device or block size has no
+// cooperative launch (the caller then launches level by level).
+template <typename MT>
+bool launch_sgs_level_coop(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* fwd_rows,
+                           const int32_t* fwd_off, int n_fwd, const int32_t* bwd_rows, const int32_t* bwd_off,
+                           int n_bwd, const double* r, double* z, const int* active, cudaStream_t s);
 void launch_krylov_init(int64_t len, const double* b, const double* v, double* r, double* r0, double* p,
                         double* partials, KrylovScalars* ks, cudaStream_t s);
 // After launch_krylov_init: a rejected initial guess (||b - A x0|| >=

@@ -463,6 +463,9 @@ void BsrSystem::build_ordering(int ordering) {
     pass_bytes(bwd_off_, br, false, bwd_bytes_, bwd_blocks_);
     upload_or_throw(fwd_rows_, fr, stream_, "sgs rows");
     upload_or_throw(bwd_rows_, br, stream_, "sgs rows");
+    upload_or_throw(fwd_off_d_, fwd_off_, stream_, "sgs levels");
+    upload_or_throw(bwd_off_d_, bwd_off_, stream_, "sgs levels");
+    cuda_check(cudaStreamSynchronize(stream_), "setup sync");  // the host vectors are rebuilt by the next call
     ordering_ = ordering;
 }
 
@@ -512,6 +515,19 @@ void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, doubl
     }
     for (int sw = 0; sw < sweeps_; ++sw) {
         const bool split = split_ && sw == 0;
+        if (!color && level_coop_) {
+            // the whole symmetric sweep as one cooperative launch
+            double bytes = 0.0;
+            for (int g = 0; g < nf; ++g) bytes += fwd_bytes_[0][g] + fwd_blocks_[0][g] * block_bytes();
+            for (int g = 0; g < nbk; ++g) bytes += bwd_bytes_[0][g] + bwd_blocks_[0][g] * block_bytes();
+            ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, bytes);
+            if (launch_sgs_level_coop<MT>(A, vals, lu, piv_.p, fwd_rows_.p, fwd_off_d_.p, nf, bwd_rows_.p,
+                                          bwd_off_d_.p, nbk, r, z, active, stream_))
+                continue;
+            cudaGetLastError();
+            level_coop_ = false;  // level by level from here on
+            --prof_->launches;
+        }
         for (int g = 0; g < nf; ++g) {
             int mode = 0;
             if (color) {
@@ -1008,9 +1024,10 @@ Solver::Solver(int device, const cfdg_mesh_host& mesh, const cfdg_config& cfg, c
     if (cfg.newton_operator != CFDG_NEWTON_PICARD && cfg.newton_operator != CFDG_NEWTON_JACOBIAN_FREE)
         throw Failure{CFDG_ERR_INVALID, "unknown Newton operator"};
     if (cfg.newton_operator == CFDG_NEWTON_JACOBIAN_FREE &&
-        (!(cfg.jf_eps > 0.0) || !(cfg.jf_rel_tol > 0.0) || cfg.jf_max_iterations < 1 || !(cfg.jf_max_change >= 0.0)))
-        throw Failure{CFDG_ERR_INVALID,
-                      "Jacobian-free Newton needs jf_eps > 0, jf_rel_tol > 0, jf_max_iterations >= 1, jf_max_change >= 0"};
+        (!(cfg.jf_eps > 0.0) || !(cfg.jf_rel_tol > 0.0) || cfg.jf_max_iterations < 1 || !(cfg.jf_max_change >= 0.0) ||
+         !(cfg.jf_accept > 0.0 && cfg.jf_accept <= 1.0)))
+        throw Failure{CFDG_ERR_INVALID, "Jacobian-free Newton needs jf_eps > 0, jf_rel_tol > 0, jf_max_iterations >= 1, "
+                                        "jf_max_change >= 0, 0 < jf_accept <= 1"};
     if (cfg.newton_operator == CFDG_NEWTON_JACOBIAN_FREE &&
         ((cfg.jf_krylov != CFDG_JF_BICGSTAB && cfg.jf_krylov != CFDG_JF_GMRES) ||
          (cfg.jf_krylov == CFDG_JF_GMRES && (cfg.jf_restart < 1 || cfg.jf_restart > 200))))
@@ -1704,7 +1721,8 @@ cfdg_krylov_result Solver::linear_solve() {
     }
     sys_->set_product(nullptr);
     const double bnorm = sys_->last_bnorm();
-    if (kr.status != CFDG_KRYLOV_DIVERGED && std::isfinite(kr.final_residual) && kr.final_residual < bnorm) {
+    if (kr.status != CFDG_KRYLOV_DIVERGED && std::isfinite(kr.final_residual) &&
+        kr.final_residual <= cfg_.jf_accept * bnorm) {
         last_jf_ = true;
         last_krylov_ = kr;
         return last_krylov_;

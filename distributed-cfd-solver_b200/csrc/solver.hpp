@@ -221,6 +221,8 @@ private:
     double block_bytes() const { return double(bs_) * bs_ * (precision_ == CFDG_PREC_MIXED ? 4.0 : 8.0); }
     bool split_ = false;  // colour-ordered matrix: first sweep split at the diagonal
     DevArray<int32_t> fwd_rows_, bwd_rows_;
+    DevArray<int32_t> fwd_off_d_, bwd_off_d_;  // level boundaries on the device (cooperative level sweep)
+    bool level_coop_ = true;                  // cleared when the cooperative launch is unavailable
     double spmv_bytes(int n_extra_vectors, bool read_y) const;
     // rows [fwd_off_[1], n) of a colour-ordered matrix: block count and
     // distinct columns (the SpMV left after the fused colour-0 product)

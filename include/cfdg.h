@@ -180,8 +180,9 @@ enum { CFDG_PREFREEZE_CONFIGURED = 0, CFDG_PREFREEZE_FP64 = 1 };
  * second-order residual, v -> (V/dt) v + (R(U + eps v) - R(U)) / eps, with
  * one eps per product that moves no conserved variable by more than
  * jf_eps of its RMS; SGS on the assembled matrix stays the preconditioner.
- * A Jacobian-free solve that does not reduce its residual is replaced by
- * the Picard solve of the same step, and a Jacobian-free step is relaxed
+ * A Jacobian-free solve that does not bring its residual below jf_accept
+ * ||b|| is replaced by the Picard solve of the same step, and a
+ * Jacobian-free step is relaxed
  * so that rho and rho E (and rho nu~, against |rho nu~| + 1e-3 of its RMS)
  * change by at most jf_max_change in any cell.  The residual, and with it
  * the converged state, is the same; only the path to it changes. */
@@ -253,6 +254,9 @@ typedef struct cfdg_config {
     double cfl_ser_max;
     int32_t jf_krylov;        /* CFDG_JF_*                                    */
     int32_t jf_restart;       /* GMRES restart length, 1..200                 */
+    /* a Jacobian-free solve is kept when its residual is at most jf_accept
+     * x ||b||; otherwise the Picard solve of the step replaces it */
+    double jf_accept;
 } cfdg_config;
 
 typedef struct cfdg_krylov_result {

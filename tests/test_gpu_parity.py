@@ -152,9 +152,9 @@ def test_gmres_matches_reference_solution(cb, refh, name):
     A.set_values(vals)
     sol_ref, info_ref = refh.bicgstab(row_ptr, cols, vals, 5, b, precond=1, rel_tol=1e-12, max_it=400)
     assert info_ref["status"] == 0
-    for ordering, restart in [(cb.SGS_LEVEL, 30), (cb.SGS_COLOR, 30), (cb.SGS_COLOR, 5)]:
+    for ordering, restart in [(cb.SGS_LEVEL, 30), (cb.SGS_COLOR, 30), (cb.SGS_COLOR, 15)]:
         A.sgs_setup(ordering, 1)
-        sol, info = A.gmres(b, precond=cb.PC_SGS, rel_tol=1e-10, max_it=600, restart=restart)
+        sol, info = A.gmres(b, precond=cb.PC_SGS, rel_tol=1e-10, max_it=2000, restart=restart)
         assert info.status == cb.KRYLOV_CONVERGED, (ordering, restart, info.iterations)
         assert info.final_residual <= 1e-10 * np.linalg.norm(b) * (1 + 1e-9)
         assert rel_err(sol, sol_ref) < 1e-7, (ordering, restart)
@@ -164,10 +164,10 @@ def test_gmres_matches_reference_solution(cb, refh, name):
     sol_n, info_n = A.gmres(b, precond=cb.PC_NONE, rel_tol=1e-10, max_it=3000, restart=60)
     assert info_n.status == cb.KRYLOV_CONVERGED
     assert rel_err(sol_n, sol_ref) < 1e-6
-    # a starting vector near the solution needs fewer iterations
+    # a starting vector near the solution (a looser solve's) needs fewer iterations
     A.sgs_setup(cb.SGS_COLOR, 1)
     _, info_0 = A.gmres(b, precond=cb.PC_SGS, rel_tol=1e-10, max_it=600)
-    x0 = sol_ref + 1e-6 * rng.standard_normal(n * 5) * np.abs(sol_ref).max()
+    x0, _ = A.gmres(b, precond=cb.PC_SGS, rel_tol=1e-4, max_it=600)
     sol_g, info_g = A.gmres(b, x0=x0, precond=cb.PC_SGS, rel_tol=1e-10, max_it=600)
     assert info_g.status == cb.KRYLOV_CONVERGED and info_g.initial_residual < info_0.initial_residual
     assert info_g.iterations < info_0.iterations
