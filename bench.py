@@ -27,8 +27,11 @@ time_to_1e8 (single GPU): the transonic Euler bump (M = 0.85; the
 default: 768,000 cells) run to a 1e-8 residual drop as plain FP64, mixed
 precision and mixed precision with the learned initial guess, each its own
 run from the free stream; converged fields are compared with the FP64 run.
-The Spalart-Allmaras plate does not reach 1e-8 with the first-order Picard
-Jacobian (the reference's method), so its time-to-1e-8 is not measured.
+time_to_1e8_plate: the laminar plate (256x128x32 hex divided by
+--plate-converge-scale, 2 by default: 131,072 cells) to 1e-8, FP64 and mixed.
+The Spalart-Allmaras plate needs tens of thousands of Newton iterations at
+full size; `--converge-only --converge-case sa_plate` runs its comparison
+(FP64, mixed, mixed + learned) at --converge-scale.
 
 `--impl reference` times the reference's CPU implementation on a bounded
 sample of the same workload (see run_reference).
@@ -510,6 +513,8 @@ def run_ours(args):
             line["cpu_baseline"] = {"value": round(v, 5), "unit": UNIT, "cores": 1, "kind": kind, "sample": desc}
         if not args.no_converge and world == 1:
             line["time_to_1e8"] = _time_to_converge(cb, args.converge_scale, not args.no_cpu_baseline)
+            line["time_to_1e8_plate"] = _time_to_converge_plate(cb, args.plate_converge_scale,
+                                                                not args.no_cpu_baseline)
         print(json.dumps(line))
     if pg is not None:
         pg.destroy_process_group()
@@ -643,6 +648,49 @@ def _time_to_converge_plate(cb, scale: int, cpu: bool = True, ser: float = 1000.
     return out
 
 
+def _time_to_converge_sa(cb, scale: int, device: int = 0):
+    """Wall time of run_steady to a 1e-8 residual drop on the
+    Spalart-Allmaras plate (384x192x56 hex divided by `scale` per direction):
+    plain FP64, mixed precision and mixed precision + learned guess (the
+    network trained first on the SA training flows), each from the free
+    stream with the Picard operator, the multicolour SGS, CFL 1->100 and the
+    limiter frozen at the ramp's end; converged rho, u, p and nu_tilde are
+    compared with the FP64 run's."""
+    net, train = _train_sa_network(cb, device)
+    case = cb.cases.sa_plate(scale=scale, iterations=60000)
+    mesh = cb.HostMesh(case.spec)
+    out = {"workload": f"Spalart-Allmaras flat plate M=0.2 Re_L=5e6, {mesh.n_cells} hex (384x192x56 / {scale}^3), "
+                       f"run_steady to a 1e-8 drop of max(mass, |momentum|, energy, nu_tilde) L2 vs its running "
+                       f"maximum",
+           "schedule": "CFL 1->100 over 50 iterations; limiter frozen at iteration 50; Picard operator, "
+                       "multicolour SGS, BiCGSTAB rtol 1e-3 max 30",
+           "training": train}
+    fields = {}
+    for name, prec, learned in (("fp64", 0, False), ("mixed", 1, False), ("mixed_learned", 1, True)):
+        c = cb.cases.sa_plate(scale=scale, iterations=60000, mixed=bool(prec))
+        with cb.Solver(mesh, c.cfg, c.bcs, device=device) as s:
+            s.init_fields()
+            if learned:
+                s.attach_guess(net)
+            r = s.run_steady()
+            fields[name] = s.get(cb.FIELD_U).reshape(6, -1)
+        out[name] = {"seconds": round(r.seconds, 3), "iterations": int(r.iterations), "converged": bool(r.converged),
+                     "rel": float(r.rel), "krylov_iterations": int(r.krylov_iterations_total)}
+    net.close()
+
+    def prim(U):
+        rho = U[0]
+        return {"rho": rho, "u": U[1] / rho, "p": 0.4 * (U[4] - 0.5 * (U[1] ** 2 + U[2] ** 2 + U[3] ** 2) / rho),
+                "nu_tilde": U[5] / rho}
+    ref = prim(fields["fp64"])
+    for name in ("mixed", "mixed_learned"):
+        q = prim(fields[name])
+        out[name]["field_rel_l2_vs_fp64"] = {
+            k: float("%.3g" % (np.linalg.norm(q[k] - ref[k]) / max(np.linalg.norm(ref[k]), 1e-300))) for k in q}
+    out["speedup_mixed_learned_vs_fp64"] = round(out["fp64"]["seconds"] / out["mixed_learned"]["seconds"], 3)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -663,9 +711,12 @@ def main():
     ap.add_argument("--converge-only", action="store_true",
                     help="run only the time-to-1e-8 comparison (one JSON line with time_to_1e8); with "
                          "--converge-scale 1 the full 6,144,000-tet bump")
-    ap.add_argument("--converge-case", default="bump", choices=["bump", "plate"],
-                    help="workload of --converge-only: the tet bump (FP64, mixed, mixed + learned) or the "
-                         "laminar plate (FP64, mixed; --converge-scale 1 = 1,048,576 cells)")
+    ap.add_argument("--converge-case", default="bump", choices=["bump", "plate", "sa_plate"],
+                    help="workload of --converge-only: the tet bump (FP64, mixed, mixed + learned), the "
+                         "laminar plate (FP64, mixed; --converge-scale 1 = 1,048,576 cells) or the SA plate "
+                         "(FP64, mixed, mixed + learned)")
+    ap.add_argument("--plate-converge-scale", type=int, default=2,
+                    help="laminar plate mesh divisor of the default run's time-to-1e-8 leg")
     ap.add_argument("--krylov-loop", default="device", choices=["device", "host"],
                     help="BiCGSTAB driver of the timed steps (host: one launch sequence per iteration, "
                          "e.g. for a profiler that does not see kernels inside conditional graph nodes)")
@@ -684,6 +735,9 @@ def main():
         if args.converge_case == "plate":
             out = _time_to_converge_plate(cb, args.converge_scale, not args.no_cpu_baseline)
             key = "time_to_1e8_plate"
+        elif args.converge_case == "sa_plate":
+            out = _time_to_converge_sa(cb, args.converge_scale)
+            key = "time_to_1e8_sa_plate"
         else:
             out = _time_to_converge(cb, args.converge_scale, not args.no_cpu_baseline)
             key = "time_to_1e8"
