@@ -393,13 +393,20 @@ __global__ void __launch_bounds__(256, (INV && BS <= 5) ? 8 : 6) k_sgs_rows(BsrV
 
 // The level-scheduled sweep (the reference's sequential order) in one
 // cooperative launch: the resident grid walks the forward levels, then the
-// backward levels, each level's rows by lane groups exactly as k_sgs_rows
-// MODE 0 with the pivoted LU, and a grid-wide barrier separates the levels
-// instead of a kernel boundary (about 1.2-1.6 us against a launch per level).
-// z entries written in one level are read by later levels on other SMs, so
-// z is read through L2 (ld.global.cg), never from a stale L1 line.  Every
-// loop is bounded by the level and row counts, and the cooperative launch
-// makes every block resident, so every barrier is reached by all blocks.
+// backward levels, with a grid-wide barrier between levels instead of a
+// kernel boundary.  A level's rows are independent but few (~1-7 thousand),
+// so the time per level is the latency of one row's dependent loads; one
+// warp takes a row and its lanes form KS = 32/BS groups of BS lanes, group
+// g computing the block products t_k = A_k[ii][:] . z_col(k) of blocks
+// k0+g, k0+g+KS, ... in parallel (one round trip for all of a row's blocks
+// instead of one per block).  Group 0 then subtracts them from r in
+// ascending block order by shuffles, which is the arithmetic of k_sgs_rows
+// MODE 0 (and of the sequential sweep) to the bit, and solves the pivoted
+// LU system.  z entries written in one level are read by later levels on
+// other SMs, so z is read through L2 (ld.global.cg), never from a stale L1
+// line.  Every loop is bounded by the level, row and block counts, and the
+// cooperative launch makes every block resident, so every barrier is
+// reached by all blocks.
 template <typename MT, int BS>
 __global__ void __launch_bounds__(256) k_sgs_level_coop(BsrView A, const MT* __restrict__ vals,
                                                         const MT* __restrict__ lu, const int8_t* __restrict__ piv,
@@ -412,12 +419,12 @@ __global__ void __launch_bounds__(256) k_sgs_level_coop(BsrView A, const MT* __r
     if (active && *active != 0) return;  // the same value for every block: all return before the first barrier
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
-    constexpr int GPW = 32 / BS;
+    constexpr int KS = 32 / BS;  // block products in flight per row
     const int lane = threadIdx.x & 31;
     const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
     const int grp = lane / BS, ii = lane - grp * BS;
-    const int base_lane = (grp < GPW ? grp : 0) * BS;
+    const bool in_grp = grp < KS;
     for (int pass = 0; pass < 2; ++pass) {
         const int32_t* rows = pass ? bwd_rows : fwd_rows;
         const int32_t* off = pass ? bwd_off : fwd_off;
@@ -425,22 +432,31 @@ __global__ void __launch_bounds__(256) k_sgs_level_coop(BsrView A, const MT* __r
         for (int g = 0; g < ng; ++g) {
             const int32_t o0 = off[g];
             const int64_t nr = off[g + 1] - o0;
-            for (int64_t first = warp * GPW; first < nr; first += nwarps * GPW) {  // warp-uniform
-                const int64_t slot = first + grp;
-                const bool act = (grp < GPW) && (slot < nr);
-                int32_t i = 0;
-                double s = 0.0;
-                if (act) {
-                    i = rows[o0 + slot];
-                    s = r[int64_t(i) * BS + ii];
-                    const int32_t d = A.diag[i];
-                    s = block_row_dot<MT, BS, true, true>(A, vals, z, ii, A.row_ptr[i], d, s);
-                    s = block_row_dot<MT, BS, true, true>(A, vals, z, ii, d + 1, A.row_ptr[i + 1], s);
+            for (int64_t slot = warp; slot < nr; slot += nwarps) {  // one row per warp: warp-uniform
+                const int32_t i = rows[o0 + slot];
+                const int32_t k0 = A.row_ptr[i], k1 = A.row_ptr[i + 1], d = A.diag[i];
+                double s = (grp == 0) ? r[int64_t(i) * BS + ii] : 0.0;
+                for (int32_t kc = k0; kc < k1; kc += KS) {  // chunks of KS blocks, warp-uniform
+                    const int32_t k = kc + grp;
+                    double t = 0.0;
+                    if (in_grp && k < k1 && k != d) {
+                        double a[BS], xb[BS];
+                        load_block_row<MT, BS>(vals + int64_t(k) * (BS * BS) + ii * BS, a);
+                        load_vec<BS, true>(z + int64_t(__ldg(A.cols + k)) * BS, xb);
+#pragma unroll
+                        for (int jj = 0; jj < BS; ++jj) t += a[jj] * xb[jj];
+                    }
+                    // ascending block order: group q holds block kc + q
+#pragma unroll
+                    for (int q = 0; q < KS; ++q) {
+                        const double tq = __shfl_sync(0xffffffffu, t, q * BS + (ii < BS ? ii : 0));
+                        if (kc + q < k1 && kc + q != d) s -= tq;
+                    }
                 }
                 double b[BS];
 #pragma unroll
-                for (int j = 0; j < BS; ++j) b[j] = __shfl_sync(0xffffffffu, s, base_lane + j);
-                if (act) {
+                for (int j = 0; j < BS; ++j) b[j] = __shfl_sync(0xffffffffu, s, j);
+                if (grp == 0) {
                     lu_solve<MT, BS>(lu + int64_t(i) * (BS * BS), piv + int64_t(i) * BS, b);
                     double out = b[0];
 #pragma unroll
