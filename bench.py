@@ -130,6 +130,7 @@ class Clocks:
 
 
 _SGS_CHOICE = "color"  # --sgs
+_NEWTON_CHOICE = "picard"  # --newton
 
 
 def _case(cb, name: str, precision: str, scale: int = 1):
@@ -148,6 +149,9 @@ def _case(cb, name: str, precision: str, scale: int = 1):
     if _SGS_CHOICE == "level":
         case.cfg.sgs_ordering = cb.SGS_LEVEL
         case.description += ", level-scheduled SGS (the reference's sweep order)"
+    if _NEWTON_CHOICE == "jf":
+        case.cfg.newton_operator = cb.NEWTON_JACOBIAN_FREE
+        case.description += ", Jacobian-free Newton-Krylov (GMRES) after the limiter freeze"
     return case
 
 
@@ -723,9 +727,13 @@ def main():
     ap.add_argument("--sgs", default="color", choices=["color", "level"],
                     help="SGS ordering of the measured legs: multicolour (default) or level-scheduled (the "
                          "reference's sequential order, one cooperative launch per sweep)")
+    ap.add_argument("--newton", default="picard", choices=["picard", "jf"],
+                    help="Newton operator of the measured legs: the assembled Picard matrix (the reference's) "
+                         "or the Jacobian-free product (profiling its kernels)")
     args = ap.parse_args()
-    global _SGS_CHOICE
+    global _SGS_CHOICE, _NEWTON_CHOICE
     _SGS_CHOICE = args.sgs
+    _NEWTON_CHOICE = args.newton
     if args.impl == "reference":
         run_reference(args)
     elif args.converge_only:
