@@ -30,6 +30,7 @@ struct DevMesh {
     const double *fdx, *fdy, *fdz, *finv_d;     // nf: face-cell distance vectors, 1/|d|
     const double *ccx, *ccy, *ccz, *vol;        // n
     const int32_t *c2f_off, *c2f;        // cell -> faces (ascending)
+    const int32_t* c2fs;                 // as c2f, ~face where the cell is the face's neighbour (the gathers' sign)
     const int32_t *c2c_off, *c2c;        // cell -> face neighbours (sorted)
     // Gradient stencil in warp slices: cells 32s..32s+31 form slice s; its
     // entries occupy slots [g_soff[s], g_soff[s+1]) with entry k of the cell

@@ -230,11 +230,12 @@ __global__ void __launch_bounds__(256) k_cell_residual(DevMesh m, DevFields f) {
     double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double l = 0.0;
     for (int32_t e = m.c2f_off[c]; e < m.c2f_off[c + 1]; ++e) {
-        const int32_t fc = m.c2f[e];
+        const int32_t es = __ldg(m.c2fs + e);  // the side is in the sign: no owner gather
+        const int32_t fc = es >= 0 ? es : ~es;
         const double2* rec = reinterpret_cast<const double2*>(f.fflux + int64_t(fc) * 6);
         const double2 a = __ldg(rec), b = __ldg(rec + 1), d = __ldg(rec + 2);
         const double F[5] = {a.x, a.y, b.x, b.y, d.x};
-        if (m.owner[fc] == c) {
+        if (es >= 0) {
 #pragma unroll
             for (int v = 0; v < 5; ++v) r[v] += F[v];
         } else {

@@ -137,9 +137,10 @@ __global__ void __launch_bounds__(128) k_sa_cell(DevMesh m, DevFields f, SaParam
     const int64_t nt = m.nt, n = m.n;
     double r = 0.0, l = f.lam[c];
     for (int32_t e = m.c2f_off[c]; e < m.c2f_off[c + 1]; ++e) {
-        const int32_t fc = m.c2f[e];
+        const int32_t es = __ldg(m.c2fs + e);  // the side is in the sign: no owner gather
+        const int32_t fc = es >= 0 ? es : ~es;
         const double2 fr = __ldg(reinterpret_cast<const double2*>(face) + fc);
-        if (m.owner[fc] == c) r += fr.x;
+        if (es >= 0) r += fr.x;
         else r -= fr.x;
         if (fc < m.ni) l += fr.y;
     }

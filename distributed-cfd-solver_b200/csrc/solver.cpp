@@ -1135,6 +1135,11 @@ void Solver::setup_mesh(const cfdg_mesh_host& mesh) {
     const Csr c2f = build_cell_faces(hm);
     upload_or_throw(c2f_off_, c2f.off, s, "c2f_off");
     upload_or_throw(c2f_, c2f.val, s, "c2f");
+    std::vector<int32_t> c2fs(c2f.val.size());
+    for (int32_t c = 0; c < n; ++c)
+        for (int32_t e = c2f.off[c]; e < c2f.off[c + 1]; ++e)
+            c2fs[e] = hm.owner[c2f.val[e]] == c ? c2f.val[e] : ~c2f.val[e];
+    upload_or_throw(c2fs_, c2fs, s, "c2fs");
     const Csr c2c = build_cell_cells_face(hm);
     upload_or_throw(c2c_off_, c2c.off, s, "c2c_off");
     upload_or_throw(c2c_, c2c.val, s, "c2c");
@@ -1171,6 +1176,7 @@ void Solver::setup_mesh(const cfdg_mesh_host& mesh) {
     dm_.vol = vol_.p;
     dm_.c2f_off = c2f_off_.p;
     dm_.c2f = c2f_.p;
+    dm_.c2fs = c2fs_.p;
     dm_.c2c_off = c2c_off_.p;
     dm_.c2c = c2c_.p;
     dm_.g_soff = g_soff_.p;
@@ -1225,7 +1231,7 @@ void Solver::compute_alg_bytes(int64_t E, int64_t n_c2c, int64_t n_c2f) {
                           : 0.0) +
                   ab_.ghost_grad;
     ab_.face_flux = F * (2 * i4 + 4 * d + 3 * d) + visc * F * 4 * d + (n + nb) * (5 + 15 + 5 + 3) * d + F * 6 * d;
-    ab_.cell_gather = (n + 1) * i4 + double(n_c2f) * i4 + F * i4 + F * 6 * d + n * 6 * d;
+    ab_.cell_gather = (n + 1) * i4 + double(n_c2f) * i4 + F * 6 * d + n * 6 * d;
     const double b2 = double(nv_) * nv_;
     const double nnzb = sys_ ? double(sys_->nnzb()) : n + 2 * Fi;
     // row-centric assembly: face owner/neigh, normal, area (+ 1/|d|), primitives

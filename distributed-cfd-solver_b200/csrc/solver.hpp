@@ -342,7 +342,7 @@ private:
     DevFields df_{};
     SaParams sap_{};
     // mesh arrays
-    DevArray<int32_t> owner_, neigh_, bpatch_, c2f_off_, c2f_, c2c_off_, c2c_, g_col_;
+    DevArray<int32_t> owner_, neigh_, bpatch_, c2f_off_, c2f_, c2fs_, c2c_off_, c2c_, g_col_;
     DevArray<int64_t> g_soff_;
     int64_t g_entries_ = 0;  // stencil entries before the slice padding
     DevArray<double> fnx_, fny_, fnz_, farea_, fcx_, fcy_, fcz_, fdx_, fdy_, fdz_, finv_d_, ccx_, ccy_, ccz_, vol_,
