@@ -9,6 +9,7 @@
 //   bsr_sgs_sweep<BS>     include/cfd/linalg/bsr_helpers.hpp:389-435
 //   BiCGSTAB::solve       src/linalg/bicgstab.cpp:42-201
 #include <algorithm>
+#include <atomic>
 
 #include <cooperative_groups.h>
 
@@ -852,20 +853,30 @@ void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const in
 #undef CFDG_SGS_M
 }
 
+// Resident 256-thread blocks of the cooperative sweep on the current device
+// (at most 4 per SM), 0 without cooperative launch; cached per device.
 template <typename MT, int BS>
 static int level_coop_grid() {
-    static int grid = -1;  // resident 256-thread blocks on every SM, once per process and instantiation
-    if (grid < 0) {
-        int dev = 0, sms = 0, per_sm = 0, coop = 0;
-        grid = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
+    constexpr int kMaxDevices = 64;
+    static std::atomic<int> cache[kMaxDevices];  // 0: unknown, -1: unavailable, else the grid
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return 0;
+    }
+    int grid = cache[dev].load();
+    if (grid == 0) {
+        int sms = 0, per_sm = 0, coop = 0;
+        grid = -1;
+        if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sgs_level_coop<MT, BS>, 256, 0) == cudaSuccess)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sgs_level_coop<MT, BS>, 256, 0) == cudaSuccess &&
+            per_sm > 0)
             grid = sms * std::min(per_sm, 4);
         cudaGetLastError();
+        cache[dev].store(grid);
     }
-    return grid;
+    return grid > 0 ? grid : 0;
 }
 
 template <typename MT>

@@ -17,6 +17,9 @@ GPU, checked through the library's own residual.
    build's converged field of the same frozen problem (FP64 level-sweep
    iterates before the freeze) to 1e-6 relative L2 on rho, u, v, p, in fewer
    Newton iterations than the Picard run.
+4. Switched evolution relaxation raises the CFL past cfl_max and lands on
+   the same converged field.
+5. Out-of-range Jacobian-free options are refused at solver creation.
 """
 import numpy as np
 import pytest
@@ -103,3 +106,32 @@ def test_ramp_jacobian_free_converges_to_the_reference_field(cb, ramp_reference,
     assert max(err.values()) < 1e-6, (err, r.iterations, it_ref)
     assert r.jacobian_free_steps > 0
     assert r.iterations < rp.iterations, (r.iterations, rp.iterations, r.picard_fallbacks)
+
+
+def test_ser_raises_the_cfl_and_keeps_the_converged_field(cb, ramp_reference):
+    """Switched evolution relaxation changes only the pseudo-time path: the
+    CFL climbs above cfl_max after the ramp and the run lands on the
+    reference's converged field of the same frozen problem."""
+    mesh, U_ref, _ = ramp_reference
+    case = cb.cases.ramp(iterations=2000)
+    case.cfg.sgs_ordering = cb.SGS_LEVEL
+    case.cfg.cfl_ser_max = 1000.0
+    with cb.Solver(mesh, case.cfg, case.bcs) as s:
+        s.init_fields()
+        r = s.run_steady()
+        U = s.get(cb.FIELD_U).reshape(5, -1)
+    assert r.converged and not r.blowup
+    assert r.cfl_last > case.cfg.cfl_max
+    err = field_errors(U, U_ref)
+    assert max(err.values()) < 1e-6, err
+
+
+@pytest.mark.parametrize("field,value", [("newton_operator", 7), ("jf_accept", 0.0), ("jf_restart", 0),
+                                         ("jf_krylov", 5), ("jf_eps", 0.0)])
+def test_jacobian_free_options_are_checked(cb, field, value):
+    case = cb.cases.ramp()
+    case.cfg.newton_operator = cb.NEWTON_JACOBIAN_FREE
+    setattr(case.cfg, field, value)
+    mesh = cb.HostMesh(case.spec)
+    with pytest.raises(cb.CfdgError):
+        cb.Solver(mesh, case.cfg, case.bcs)
