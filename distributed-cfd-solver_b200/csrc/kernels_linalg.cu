@@ -238,6 +238,10 @@ __global__ void __launch_bounds__(kLuThreads, BS == 6 ? 3 : 4) k_lu(BsrView A, c
     __syncthreads();  // every thread has read its block
     if (act) {
         if constexpr (INV) {
+            // the U diagonal's reciprocals once: BS divisions instead of BS*BS
+            double rd[BS];
+#pragma unroll
+            for (int r = 0; r < BS; ++r) rd[r] = 1.0 / a[r * BS + r];
 #pragma unroll
             for (int c = 0; c < BS; ++c) {
                 double x[BS];
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(kLuThreads, BS == 6 ? 3 : 4) k_lu(BsrView A, c
                 for (int r = BS - 1; r >= 0; --r) {
 #pragma unroll
                     for (int j = r + 1; j < BS; ++j) x[r] -= a[r * BS + j] * x[j];
-                    x[r] = x[r] / a[r * BS + r];
+                    x[r] = x[r] * rd[r];
                 }
 #pragma unroll
                 for (int r = 0; r < BS; ++r) sm[threadIdx.x * SP + r * BS + c] = static_cast<MT>(x[r]);
@@ -408,12 +412,16 @@ __global__ void __launch_bounds__(256, (INV && BS <= 5) ? 8 : 6) k_sgs_rows(BsrV
 // line.  Every loop is bounded by the level, row and block counts, and the
 // cooperative launch makes every block resident, so every barrier is
 // reached by all blocks.
+// `fwd_rows` / `bwd_rows` are the passes' rows in level order as int4
+// records (row, first block, end of the row's blocks, diagonal block), so a
+// row's structure is one 16-byte load rather than a row-list load followed
+// by the row-pointer and diagonal loads.
 template <typename MT, int BS>
 __global__ void __launch_bounds__(256) k_sgs_level_coop(BsrView A, const MT* __restrict__ vals,
                                                         const MT* __restrict__ lu, const int8_t* __restrict__ piv,
-                                                        const int32_t* __restrict__ fwd_rows,
+                                                        const int4* __restrict__ fwd_rows,
                                                         const int32_t* __restrict__ fwd_off, int n_fwd,
-                                                        const int32_t* __restrict__ bwd_rows,
+                                                        const int4* __restrict__ bwd_rows,
                                                         const int32_t* __restrict__ bwd_off, int n_bwd,
                                                         const double* __restrict__ r, double* z,
                                                         const int* __restrict__ active) {
@@ -427,15 +435,15 @@ __global__ void __launch_bounds__(256) k_sgs_level_coop(BsrView A, const MT* __r
     const int grp = lane / BS, ii = lane - grp * BS;
     const bool in_grp = grp < KS;
     for (int pass = 0; pass < 2; ++pass) {
-        const int32_t* rows = pass ? bwd_rows : fwd_rows;
+        const int4* rows = pass ? bwd_rows : fwd_rows;
         const int32_t* off = pass ? bwd_off : fwd_off;
         const int ng = pass ? n_bwd : n_fwd;
         for (int g = 0; g < ng; ++g) {
             const int32_t o0 = off[g];
             const int64_t nr = off[g + 1] - o0;
             for (int64_t slot = warp; slot < nr; slot += nwarps) {  // one row per warp: warp-uniform
-                const int32_t i = rows[o0 + slot];
-                const int32_t k0 = A.row_ptr[i], k1 = A.row_ptr[i + 1], d = A.diag[i];
+                const int4 rec = __ldg(rows + o0 + slot);
+                const int32_t i = rec.x, k0 = rec.y, k1 = rec.z, d = rec.w;
                 double s = (grp == 0) ? r[int64_t(i) * BS + ii] : 0.0;
                 for (int32_t kc = k0; kc < k1; kc += KS) {  // chunks of KS blocks, warp-uniform
                     const int32_t k = kc + grp;
@@ -880,8 +888,8 @@ static int level_coop_grid() {
 }
 
 template <typename MT>
-bool launch_sgs_level_coop(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* fwd_rows,
-                           const int32_t* fwd_off, int n_fwd, const int32_t* bwd_rows, const int32_t* bwd_off,
+bool launch_sgs_level_coop(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int4* fwd_rows,
+                           const int32_t* fwd_off, int n_fwd, const int4* bwd_rows, const int32_t* bwd_off,
                            int n_bwd, const double* r, double* z, const int* active, cudaStream_t s) {
     void* args[] = {const_cast<BsrView*>(&A), &vals, &lu, &piv, &fwd_rows, &fwd_off, &n_fwd, &bwd_rows, &bwd_off,
                     &n_bwd, &r, &z, &active};
@@ -955,10 +963,10 @@ template void launch_sgs_last_spmv<float>(const BsrView&, const float*, const fl
 template void launch_lu_setup<double>(const BsrView&, const double*, double*, int8_t*, int*, bool, cudaStream_t);
 template void launch_lu_setup<float>(const BsrView&, const float*, float*, int8_t*, int*, bool, cudaStream_t);
 template bool launch_sgs_level_coop<double>(const BsrView&, const double*, const double*, const int8_t*,
-                                            const int32_t*, const int32_t*, int, const int32_t*, const int32_t*, int,
+                                            const int4*, const int32_t*, int, const int4*, const int32_t*, int,
                                             const double*, double*, const int*, cudaStream_t);
-template bool launch_sgs_level_coop<float>(const BsrView&, const float*, const float*, const int8_t*, const int32_t*,
-                                           const int32_t*, int, const int32_t*, const int32_t*, int, const double*,
+template bool launch_sgs_level_coop<float>(const BsrView&, const float*, const float*, const int8_t*, const int4*,
+                                           const int32_t*, int, const int4*, const int32_t*, int, const double*,
                                            double*, const int*, cudaStream_t);
 template void launch_sgs_rows_ex<double>(const BsrView&, const double*, const double*, const int8_t*, const int32_t*,
                                          int32_t, int32_t, const double*, double*, int, bool, const int*,

@@ -57,11 +57,12 @@ void launch_sgs_rows_ex(const BsrView& A, const MT* vals, const MT* lu, const in
                         const int* active, cudaStream_t s);
 // The whole level-scheduled symmetric sweep (forward levels, then backward
 // levels; z zeroed by the caller) as one cooperative launch with a grid
-// barrier per level; false when the device or block size has no
+// barrier per level; rows as (row, row_ptr[row], row_ptr[row+1], diag[row])
+// records in level order.  False when the device or block size has no
 // cooperative launch (the caller then launches level by level).
 template <typename MT>
-bool launch_sgs_level_coop(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int32_t* fwd_rows,
-                           const int32_t* fwd_off, int n_fwd, const int32_t* bwd_rows, const int32_t* bwd_off,
+bool launch_sgs_level_coop(const BsrView& A, const MT* vals, const MT* lu, const int8_t* piv, const int4* fwd_rows,
+                           const int32_t* fwd_off, int n_fwd, const int4* bwd_rows, const int32_t* bwd_off,
                            int n_bwd, const double* r, double* z, const int* active, cudaStream_t s);
 void launch_krylov_init(int64_t len, const double* b, const double* v, double* r, double* r0, double* p,
                         double* partials, KrylovScalars* ks, cudaStream_t s);

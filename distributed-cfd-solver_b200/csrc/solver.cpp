@@ -465,6 +465,18 @@ void BsrSystem::build_ordering(int ordering) {
     upload_or_throw(bwd_rows_, br, stream_, "sgs rows");
     upload_or_throw(fwd_off_d_, fwd_off_, stream_, "sgs levels");
     upload_or_throw(bwd_off_d_, bwd_off_, stream_, "sgs levels");
+    if (ordering == CFDG_SGS_LEVEL) {
+        auto meta = [&](const std::vector<int32_t>& rows) {
+            std::vector<int4> m(rows.size());
+            for (std::size_t q = 0; q < rows.size(); ++q) {
+                const int32_t i = rows[q];
+                m[q] = make_int4(i, row_ptr_h_[i], row_ptr_h_[i + 1], diag_h_[i]);
+            }
+            return m;
+        };
+        upload_or_throw(fwd_meta_, meta(fr), stream_, "sgs level rows");
+        upload_or_throw(bwd_meta_, meta(br), stream_, "sgs level rows");
+    }
     cuda_check(cudaStreamSynchronize(stream_), "setup sync");  // the host vectors are rebuilt by the next call
     ordering_ = ordering;
 }
@@ -521,7 +533,8 @@ void BsrSystem::sgs_apply_t(const MT* vals, const MT* lu, const double* r, doubl
             for (int g = 0; g < nf; ++g) bytes += fwd_bytes_[0][g] + fwd_blocks_[0][g] * block_bytes();
             for (int g = 0; g < nbk; ++g) bytes += bwd_bytes_[0][g] + bwd_blocks_[0][g] * block_bytes();
             ProfScope ps(prof_, CFDG_KCAT_SGS, stream_, 1, bytes);
-            if (launch_sgs_level_coop<MT>(A, vals, lu, piv_.p, fwd_rows_.p, fwd_off_d_.p, nf, bwd_rows_.p,
+            if (fwd_meta_.p &&
+                launch_sgs_level_coop<MT>(A, vals, lu, piv_.p, fwd_meta_.p, fwd_off_d_.p, nf, bwd_meta_.p,
                                           bwd_off_d_.p, nbk, r, z, active, stream_))
                 continue;
             cudaGetLastError();

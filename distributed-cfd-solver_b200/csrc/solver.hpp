@@ -222,6 +222,7 @@ private:
     bool split_ = false;  // colour-ordered matrix: first sweep split at the diagonal
     DevArray<int32_t> fwd_rows_, bwd_rows_;
     DevArray<int32_t> fwd_off_d_, bwd_off_d_;  // level boundaries on the device (cooperative level sweep)
+    DevArray<int4> fwd_meta_, bwd_meta_;       // (row, first block, block end, diagonal) in level order
     bool level_coop_ = true;                  // cleared when the cooperative launch is unavailable
     double spmv_bytes(int n_extra_vectors, bool read_y) const;
     // rows [fwd_off_[1], n) of a colour-ordered matrix: block count and
