@@ -49,6 +49,9 @@ KRYLOV_DEVICE_LOOP, KRYLOV_HOST_LOOP = 0, 1
 PREFREEZE_CONFIGURED, PREFREEZE_FP64 = 0, 1
 TIME_STEADY, TIME_UNSTEADY = 0, 1
 NEWTON_PICARD, NEWTON_JACOBIAN_FREE = 0, 1
+# cfdg_halo_get arrays (CFDG_HALO_*)
+CFDG_HALO_ARRAYS = {"local_to_global": 0, "nb_ranks": 1, "send_offsets": 2, "send_owned_local": 3,
+                    "recv_offsets": 4, "recv_ghost_local": 5}
 JF_BICGSTAB, JF_GMRES = 0, 1
 STAGE_PRIMITIVES, STAGE_GRADIENT, STAGE_LIMITER, STAGE_FLUXES = range(4)
 KCAT_NAMES = ("primitives", "gradient", "limiter", "face_flux", "cell_gather", "jacobian", "lu", "spmv", "sgs",
@@ -206,6 +209,12 @@ _SIGS = {
                                 C.POINTER(C.c_void_p), C.c_int32, C.c_void_p]),
     "cfdg_limiter": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32, C.c_void_p]),
+    "cfdg_halo_create": (C.c_int, [C.POINTER(MeshHost), C.c_int32, _ip, C.c_int32, C.POINTER(C.c_void_p)]),
+    "cfdg_halo_destroy": (C.c_int, [C.c_void_p]),
+    "cfdg_halo_sizes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "cfdg_halo_get": (C.c_int, [C.c_void_p, C.c_int32, _ip, C.c_int64]),
+    "cfdg_halo_pack": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.c_int32, C.c_void_p, C.c_void_p]),
+    "cfdg_halo_unpack": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.c_void_p]),
     "cfdg_bsr_create": (C.c_int, [C.c_int, C.c_int32, C.c_int32, _ip, _ip, C.c_int32, C.POINTER(C.c_void_p)]),
     "cfdg_bsr_destroy": (C.c_int, [C.c_void_p]),
     "cfdg_bsr_set_values": (C.c_int, [C.c_void_p, _dp]),
@@ -362,6 +371,10 @@ class HostMesh:
                   "face_normal_z", "face_area"):
             out[k] = _np(getattr(v, k), nf, np.float64)
         return out
+
+
+def _dptr_int(a: np.ndarray):
+    return a.ctypes.data_as(_ip)
 
 
 def _dptr(a: np.ndarray):
@@ -726,3 +739,4 @@ class Bsr:
 
 
 from . import cases  # noqa: E402,F401  (benchmark workloads)
+from . import halo  # noqa: E402,F401  (partitions and halo exchange)

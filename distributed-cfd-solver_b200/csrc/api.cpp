@@ -9,6 +9,7 @@
 #include <string>
 
 #include "cfdg.h"
+#include "halo.hpp"
 #include "host_mesh.hpp"
 #include "recon.hpp"
 #include "solver.hpp"
@@ -36,6 +37,9 @@ struct cfdg_dataset {
 };
 struct cfdg_recon {
     cfdg::ReconOperator* impl;
+};
+struct cfdg_halo {
+    cfdg::HaloPlan plan;
 };
 
 namespace cfdg {
@@ -81,6 +85,32 @@ int require_device(int device) {
     return CFDG_OK;
 }
 
+}  // namespace
+
+namespace {
+// uploads the plan's index lists to `device` on first use
+int halo_device_ready(cfdg_halo* h, int device, int32_t nvars) {
+    if (nvars < 1 || nvars > cfdg::kHaloMaxVars) {
+        cfdg::set_error("halo: nvars must be in [1, 32]");
+        return CFDG_ERR_INVALID;
+    }
+    const int dv = require_device(device);
+    if (dv != CFDG_OK) return dv;
+    cfdg::HaloPlan& p = h->plan;
+    if (p.device >= 0 && p.device != device) {
+        cfdg::set_error("halo: the plan's index lists live on another device");
+        return CFDG_ERR_INVALID;
+    }
+    return guarded([&] {
+        cfdg::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        if (p.device < 0) {
+            cfdg::upload_or_throw(p.send_d, p.send_owned_local, nullptr, "halo send list");
+            cfdg::upload_or_throw(p.recv_d, p.recv_ghost_local, nullptr, "halo recv list");
+            cfdg::cuda_check(cudaStreamSynchronize(nullptr), "halo upload");
+            p.device = device;
+        }
+    });
+}
 }  // namespace
 
 extern "C" {
@@ -734,6 +764,93 @@ int cfdg_limiter(cfdg_recon* r, const double* const* q_d, const double* const* g
                  const double* const* gz_d, double* const* phi_d, int32_t nvars, void* stream) {
     if (!r || !r->impl) return CFDG_ERR_INVALID;
     return guarded([&] { r->impl->limiter(q_d, gx_d, gy_d, gz_d, phi_d, nvars, static_cast<cudaStream_t>(stream)); });
+}
+
+// ------------------------------------------------------ partitions and halos
+int cfdg_halo_create(const cfdg_mesh_host* mesh_h, int32_t nparts, const int32_t* part_h, int32_t rank,
+                     cfdg_halo** out) {
+    if (!mesh_h || !out) return CFDG_ERR_INVALID;
+    *out = nullptr;
+    return guarded([&] {
+        cfdg::HostMesh hm;
+        hm.from_view(*mesh_h);
+        auto* h = new cfdg_halo{};
+        try {
+            cfdg::build_halo_plan(hm, nparts, part_h, rank, h->plan);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int cfdg_halo_destroy(cfdg_halo* h) {
+    if (!h) return CFDG_OK;
+    if (h->plan.device >= 0) cudaSetDevice(h->plan.device);
+    delete h;
+    return CFDG_OK;
+}
+
+int cfdg_halo_sizes(const cfdg_halo* h, int64_t* sizes_h) {
+    if (!h || !sizes_h) return CFDG_ERR_INVALID;
+    const cfdg::HaloPlan& p = h->plan;
+    sizes_h[0] = p.n_own;
+    sizes_h[1] = p.n_local;
+    sizes_h[2] = static_cast<int64_t>(p.nb_ranks.size());
+    sizes_h[3] = static_cast<int64_t>(p.send_owned_local.size());
+    sizes_h[4] = static_cast<int64_t>(p.recv_ghost_local.size());
+    return CFDG_OK;
+}
+
+int cfdg_halo_get(const cfdg_halo* h, int32_t what, int32_t* out_h, int64_t count) {
+    if (!h || !out_h) return CFDG_ERR_INVALID;
+    const cfdg::HaloPlan& p = h->plan;
+    const std::vector<int32_t>* v = nullptr;
+    switch (what) {
+        case CFDG_HALO_LOCAL_TO_GLOBAL: v = &p.local_to_global; break;
+        case CFDG_HALO_NB_RANKS: v = &p.nb_ranks; break;
+        case CFDG_HALO_SEND_OFFSETS: v = &p.send_offsets; break;
+        case CFDG_HALO_SEND_OWNED_LOCAL: v = &p.send_owned_local; break;
+        case CFDG_HALO_RECV_OFFSETS: v = &p.recv_offsets; break;
+        case CFDG_HALO_RECV_GHOST_LOCAL: v = &p.recv_ghost_local; break;
+        default: cfdg::set_error("unknown halo array"); return CFDG_ERR_INVALID;
+    }
+    if (count < static_cast<int64_t>(v->size())) {
+        cfdg::set_error("output buffer too small");
+        return CFDG_ERR_INVALID;
+    }
+    std::copy(v->begin(), v->end(), out_h);
+    return CFDG_OK;
+}
+
+
+int cfdg_halo_pack(cfdg_halo* h, int device, const double* const* fields_d, int32_t nvars, double* send_d,
+                   void* stream) {
+    if (!h || !fields_d || (!send_d && !h->plan.send_owned_local.empty())) return CFDG_ERR_INVALID;
+    const int st = halo_device_ready(h, device, nvars);
+    if (st != CFDG_OK) return st;
+    return guarded([&] {
+        cfdg::HaloFields f{};
+        for (int v = 0; v < nvars; ++v) f.p[v] = const_cast<double*>(fields_d[v]);
+        cfdg::launch_halo_pack(static_cast<int32_t>(h->plan.send_owned_local.size()), h->plan.send_d.p, f, nvars,
+                               send_d, static_cast<cudaStream_t>(stream));
+        cfdg::cuda_check(cudaGetLastError(), "halo pack launch");
+    });
+}
+
+int cfdg_halo_unpack(cfdg_halo* h, int device, const double* recv_d, int32_t nvars, double* const* fields_d,
+                     void* stream) {
+    if (!h || !fields_d || (!recv_d && !h->plan.recv_ghost_local.empty())) return CFDG_ERR_INVALID;
+    const int st = halo_device_ready(h, device, nvars);
+    if (st != CFDG_OK) return st;
+    return guarded([&] {
+        cfdg::HaloFields f{};
+        for (int v = 0; v < nvars; ++v) f.p[v] = fields_d[v];
+        cfdg::launch_halo_unpack(static_cast<int32_t>(h->plan.recv_ghost_local.size()), h->plan.recv_d.p, recv_d,
+                                 nvars, f, static_cast<cudaStream_t>(stream));
+        cfdg::cuda_check(cudaGetLastError(), "halo unpack launch");
+    });
 }
 
 }  // extern "C"

@@ -523,6 +523,44 @@ CFDG_API int cfdg_dataset_read_host(const cfdg_dataset* d, uint16_t* x_h, float*
 CFDG_API int cfdg_solver_attach_guess(cfdg_solver* s, cfdg_mlp* m);
 CFDG_API int cfdg_solver_attach_dataset(cfdg_solver* s, cfdg_dataset* d, int32_t stride);
 
+/* ---------------------------------------------------- partitions and halos
+ * The halo fields of mesh::MeshPart (include/cfd/mesh/localmesh.hpp:30-32,
+ * 79-83) for one rank of a partitioned mesh, and the device side of
+ * HaloExchanger (src/fields/halo.cpp:212-330): pack the listed owned
+ * cells of SoA fields into one AoS message (nvars values a cell, one group
+ * a neighbour, in plan order) and scatter a received message into the
+ * ghost cells.  The transport of the messages is the caller's (NCCL
+ * send/recv, e.g. through torch.distributed); the solver itself runs one
+ * partition (n_own == n_cells).
+ * part_h[c]: the rank owning global cell c, or NULL for nparts contiguous
+ * ranges of the cell order.  Local cells: the owned cells in ascending
+ * global order, then the ghosts grouped by owning rank (ascending) and
+ * ascending in global id; a sender's group for rank r lists the same cells
+ * in the same order as r's group for the sender.  Host only until the
+ * first pack/unpack, which uploads the index lists to `device`. */
+typedef struct cfdg_halo cfdg_halo;
+enum {
+    CFDG_HALO_LOCAL_TO_GLOBAL = 0,   /* n_local                                */
+    CFDG_HALO_NB_RANKS = 1,          /* n_neighbours                           */
+    CFDG_HALO_SEND_OFFSETS = 2,      /* n_neighbours + 1                       */
+    CFDG_HALO_SEND_OWNED_LOCAL = 3,  /* n_send: local indices in [0, n_own)     */
+    CFDG_HALO_RECV_OFFSETS = 4,      /* n_neighbours + 1                       */
+    CFDG_HALO_RECV_GHOST_LOCAL = 5   /* n_recv: local indices in [n_own, n_local) */
+};
+CFDG_API int cfdg_halo_create(const cfdg_mesh_host* mesh_h, int32_t nparts, const int32_t* part_h, int32_t rank,
+                              cfdg_halo** out);
+CFDG_API int cfdg_halo_destroy(cfdg_halo* h);
+/* sizes_h[5] = {n_own, n_local, n_neighbours, n_send, n_recv} */
+CFDG_API int cfdg_halo_sizes(const cfdg_halo* h, int64_t* sizes_h);
+CFDG_API int cfdg_halo_get(const cfdg_halo* h, int32_t what, int32_t* out_h, int64_t count);
+/* send_d[i*nvars + v] = fields_d[v][send_owned_local[i]], i < n_send;
+ * fields_d is a host array of nvars (<= 32) device pointers */
+CFDG_API int cfdg_halo_pack(cfdg_halo* h, int device, const double* const* fields_d, int32_t nvars, double* send_d,
+                            void* stream);
+/* fields_d[v][recv_ghost_local[i]] = recv_d[i*nvars + v], i < n_recv */
+CFDG_API int cfdg_halo_unpack(cfdg_halo* h, int device, const double* recv_d, int32_t nvars,
+                              double* const* fields_d, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
