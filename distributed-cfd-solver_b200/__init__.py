@@ -215,6 +215,8 @@ _SIGS = {
     "cfdg_halo_get": (C.c_int, [C.c_void_p, C.c_int32, _ip, C.c_int64]),
     "cfdg_halo_pack": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.c_int32, C.c_void_p, C.c_void_p]),
     "cfdg_halo_unpack": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.c_void_p]),
+    "cfdg_halo_pack_blocks": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "cfdg_halo_unpack_blocks": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "cfdg_bsr_create": (C.c_int, [C.c_int, C.c_int32, C.c_int32, _ip, _ip, C.c_int32, C.POINTER(C.c_void_p)]),
     "cfdg_bsr_destroy": (C.c_int, [C.c_void_p]),
     "cfdg_bsr_set_values": (C.c_int, [C.c_void_p, _dp]),

@@ -91,7 +91,7 @@ namespace {
 // uploads the plan's index lists to `device` on first use
 int halo_device_ready(cfdg_halo* h, int device, int32_t nvars) {
     if (nvars < 1 || nvars > cfdg::kHaloMaxVars) {
-        cfdg::set_error("halo: nvars must be in [1, 32]");
+        cfdg::set_error("halo: nvars (or the block size) must be in [1, 32]");
         return CFDG_ERR_INVALID;
     }
     const int dv = require_device(device);
@@ -849,6 +849,28 @@ int cfdg_halo_unpack(cfdg_halo* h, int device, const double* recv_d, int32_t nva
         for (int v = 0; v < nvars; ++v) f.p[v] = fields_d[v];
         cfdg::launch_halo_unpack(static_cast<int32_t>(h->plan.recv_ghost_local.size()), h->plan.recv_d.p, recv_d,
                                  nvars, f, static_cast<cudaStream_t>(stream));
+        cfdg::cuda_check(cudaGetLastError(), "halo unpack launch");
+    });
+}
+
+int cfdg_halo_pack_blocks(cfdg_halo* h, int device, const double* x_d, int32_t bs, double* send_d, void* stream) {
+    if (!h || !x_d || (!send_d && !h->plan.send_owned_local.empty())) return CFDG_ERR_INVALID;
+    const int st = halo_device_ready(h, device, bs);
+    if (st != CFDG_OK) return st;
+    return guarded([&] {
+        cfdg::launch_halo_pack_blocks(static_cast<int32_t>(h->plan.send_owned_local.size()), h->plan.send_d.p, x_d,
+                                      bs, send_d, static_cast<cudaStream_t>(stream));
+        cfdg::cuda_check(cudaGetLastError(), "halo pack launch");
+    });
+}
+
+int cfdg_halo_unpack_blocks(cfdg_halo* h, int device, const double* recv_d, int32_t bs, double* x_d, void* stream) {
+    if (!h || !x_d || (!recv_d && !h->plan.recv_ghost_local.empty())) return CFDG_ERR_INVALID;
+    const int st = halo_device_ready(h, device, bs);
+    if (st != CFDG_OK) return st;
+    return guarded([&] {
+        cfdg::launch_halo_unpack_blocks(static_cast<int32_t>(h->plan.recv_ghost_local.size()), h->plan.recv_d.p,
+                                        recv_d, bs, x_d, static_cast<cudaStream_t>(stream));
         cfdg::cuda_check(cudaGetLastError(), "halo unpack launch");
     });
 }

@@ -40,5 +40,8 @@ struct HaloFields {
 void launch_halo_pack(int32_t n, const int32_t* idx, const HaloFields& f, int nvars, double* msg, cudaStream_t s);
 void launch_halo_unpack(int32_t n, const int32_t* idx, const double* msg, int nvars, const HaloFields& f,
                         cudaStream_t s);
+// The same for a block vector x[row * bs + v] (bs <= kHaloMaxVars).
+void launch_halo_pack_blocks(int32_t n, const int32_t* idx, const double* x, int bs, double* msg, cudaStream_t s);
+void launch_halo_unpack_blocks(int32_t n, const int32_t* idx, const double* msg, int bs, double* x, cudaStream_t s);
 
 }  // namespace cfdg

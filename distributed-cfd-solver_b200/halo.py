@@ -81,21 +81,44 @@ class HaloPlan:
         check(lib().cfdg_halo_unpack(self._h, device, C.c_void_p(int(recv)), len(fields), _ptr_array(fields),
                                      C.c_void_p(stream or None)))
 
+    def pack_blocks(self, x, bs: int, send, device: int, stream: int = 0):
+        """send[i*bs + v] = x[send_owned_local[i]*bs + v] (a block vector, device addresses)."""
+        check(lib().cfdg_halo_pack_blocks(self._h, device, C.c_void_p(int(x)), bs, C.c_void_p(int(send)),
+                                          C.c_void_p(stream or None)))
 
-def _device_packer(plan: HaloPlan):
-    """Pack/unpack of CUDA tensors through the library's kernels on the
-    current torch stream."""
-    import torch
+    def unpack_blocks(self, recv, bs: int, x, device: int, stream: int = 0):
+        """x[recv_ghost_local[i]*bs + v] = recv[i*bs + v] (a block vector, device addresses)."""
+        check(lib().cfdg_halo_unpack_blocks(self._h, device, C.c_void_p(int(recv)), bs, C.c_void_p(int(x)),
+                                            C.c_void_p(stream or None)))
 
-    def pack(fields, send):
-        dev = send.device.index
-        plan.pack([f.data_ptr() for f in fields], send.data_ptr(), dev, torch.cuda.current_stream(dev).cuda_stream)
 
-    def unpack(recv, fields):
-        dev = recv.device.index
-        plan.unpack(recv.data_ptr(), [f.data_ptr() for f in fields], dev,
-                    torch.cuda.current_stream(dev).cuda_stream)
-    return pack, unpack
+class DevicePacker:
+    """Message packing of CUDA tensors by the library's kernels on the
+    current torch stream: fields (SoA phases) and block vectors."""
+
+    def __init__(self, plan: HaloPlan):
+        self.plan = plan
+
+    @staticmethod
+    def _stream(t):
+        import torch
+        return t.device.index, torch.cuda.current_stream(t.device.index).cuda_stream
+
+    def pack(self, fields, send):
+        dev, st = self._stream(send)
+        self.plan.pack([f.data_ptr() for f in fields], send.data_ptr(), dev, st)
+
+    def unpack(self, recv, fields):
+        dev, st = self._stream(recv)
+        self.plan.unpack(recv.data_ptr(), [f.data_ptr() for f in fields], dev, st)
+
+    def pack_blocks(self, x, bs, send):
+        dev, st = self._stream(send)
+        self.plan.pack_blocks(x.data_ptr(), bs, send.data_ptr(), dev, st)
+
+    def unpack_blocks(self, recv, bs, x):
+        dev, st = self._stream(recv)
+        self.plan.unpack_blocks(recv.data_ptr(), bs, x.data_ptr(), dev, st)
 
 
 class HaloExchanger:
@@ -104,16 +127,21 @@ class HaloExchanger:
     Fields are 1-D float64 tensors of at least plan.n_local entries (local
     cell order), on the device the library packs them on.  `group` is the
     torch.distributed process group (None: the default one).  `packer`
-    replaces the device pack/unpack pair (pack(fields, send_tensor),
-    unpack(recv_tensor, fields)); the default runs the library's kernels
-    and needs CUDA tensors."""
+    replaces the device packing (an object with pack(fields, send),
+    unpack(recv, fields), pack_blocks(x, bs, send), unpack_blocks(recv, bs,
+    x)); the default, DevicePacker, runs the library's kernels and needs
+    CUDA tensors."""
 
-    FIELD_TAG, GRAD_LIMITER_TAG, ONCE_TAG = 4242, 4243, 4244  # the reference's message tags
+    # the reference's message tags: cell fields, gradients + limiters,
+    # one-off groups (src/fields/halo.cpp:16-18), block vectors
+    # (vector_layout.hpp:215)
+    FIELD_TAG, GRAD_LIMITER_TAG, ONCE_TAG, VECTOR_TAG = 4242, 4243, 4244, 4317
 
     def __init__(self, plan: HaloPlan, group=None, packer=None):
         self.plan = plan
         self.group = group
-        self._pack, self._unpack = packer if packer is not None else _device_packer(plan)
+        self.packer = packer if packer is not None else DevicePacker(plan)
+        self._pack, self._unpack = self.packer.pack, self.packer.unpack
         self._phases = {"fields": {"ptrs": [], "tag": self.FIELD_TAG},
                         "grads": {"ptrs": [], "tag": self.GRAD_LIMITER_TAG}}
 
@@ -152,13 +180,15 @@ class HaloExchanger:
         return len(self._phases["grads"]["ptrs"])
 
     # one phase: post receives, pack and send, then wait and unpack
-    def _start(self, ph):
+    def _start(self, ph, nv=None, packed=False):
         import torch.distributed as dist
         p = self.plan
         if not p.nb_ranks.size or not ph["ptrs"]:
             return
-        nv = len(ph["ptrs"])
-        self._pack(ph["ptrs"], ph["send"])
+        if nv is None:
+            nv = len(ph["ptrs"])
+        if not packed:
+            self._pack(ph["ptrs"], ph["send"])
         ops = []
         for k, r in enumerate(p.nb_ranks):
             r0, r1 = int(p.recv_offsets[k]) * nv, int(p.recv_offsets[k + 1]) * nv
@@ -168,14 +198,15 @@ class HaloExchanger:
             ops.append(dist.P2POp(dist.isend, ph["send"][s0:s1], int(r), self.group, ph["tag"]))
         ph["reqs"] = dist.batch_isend_irecv(ops)
 
-    def _finish(self, ph):
+    def _finish(self, ph, unpack=True):
         p = self.plan
         if not p.nb_ranks.size or not ph["ptrs"]:
             return
         for q in ph["reqs"]:
             q.wait()
         ph["reqs"] = []
-        self._unpack(ph["recv"], ph["ptrs"])
+        if unpack:
+            self._unpack(ph["recv"], ph["ptrs"])
 
     def start_exchange_fields(self):
         self._start(self._phases["fields"])
@@ -206,6 +237,26 @@ class HaloExchanger:
         self._resize(ph)
         self._start(ph)
         self._finish(ph)
+
+
+    def exchange_vector(self, x, bs: int):
+        """Ghost rows of a block vector x[row*bs + v] (n_local rows, the
+        Krylov vectors' layout) from their owners: the reference vector
+        layout's pack_values, post_sr and wait_and_unpack
+        (include/cfd/linalg/vector_layout.hpp:172-260)."""
+        import torch
+        p = self.plan
+        if not p.nb_ranks.size:
+            return
+        if x.dim() != 1 or x.numel() < p.n_local * bs:
+            raise ValueError("the vector needs n_local * bs entries")
+        ph = {"ptrs": [x], "tag": self.VECTOR_TAG, "reqs": [],
+              "send": torch.zeros(p.n_send * bs, dtype=torch.float64, device=x.device),
+              "recv": torch.zeros(p.n_recv * bs, dtype=torch.float64, device=x.device)}
+        self.packer.pack_blocks(x, bs, ph["send"])
+        self._start(ph, nv=bs, packed=True)
+        self._finish(ph, unpack=False)
+        self.packer.unpack_blocks(ph["recv"], bs, x)
 
 
 def allreduce_sum(values, group=None):

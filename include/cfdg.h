@@ -560,6 +560,14 @@ CFDG_API int cfdg_halo_pack(cfdg_halo* h, int device, const double* const* field
 /* fields_d[v][recv_ghost_local[i]] = recv_d[i*nvars + v], i < n_recv */
 CFDG_API int cfdg_halo_unpack(cfdg_halo* h, int device, const double* recv_d, int32_t nvars,
                               double* const* fields_d, void* stream);
+/* The same for a block vector x_d[row*bs + v] (n_local rows, local order;
+ * the Krylov vectors' layout, vector_layout.hpp:170-250), bs in [1, 32]:
+ * send_d[i*bs + v] = x_d[send_owned_local[i]*bs + v] and
+ * x_d[recv_ghost_local[i]*bs + v] = recv_d[i*bs + v]. */
+CFDG_API int cfdg_halo_pack_blocks(cfdg_halo* h, int device, const double* x_d, int32_t bs, double* send_d,
+                                   void* stream);
+CFDG_API int cfdg_halo_unpack_blocks(cfdg_halo* h, int device, const double* recv_d, int32_t bs, double* x_d,
+                                     void* stream);
 
 #ifdef __cplusplus
 }

@@ -58,3 +58,32 @@ def test_pack_matches_the_numpy_restatement(cb):
     assert np.array_equal(send.cpu().numpy(), want)
     with pytest.raises(cb.CfdgError):  # more variables than a message holds
         p.pack([dev[0].data_ptr()] * 33, send.data_ptr(), 0)
+
+
+def test_block_vector_pack_route_unpack(cb):
+    """The Krylov-layout form (x[row*bs + v]): rows packed by the owners
+    and unpacked into the receivers' ghost rows."""
+    import torch
+    mesh = cb.HostMesh(cb.cases.bump(scale=16).spec)
+    nparts, bs = 3, 6
+    plans = [cb.halo.HaloPlan(mesh, nparts, r) for r in range(nparts)]
+    xs, sends = [], []
+    for p in plans:
+        g = p.local_to_global.astype(np.float64)
+        want = (g[:, None] * 10.0 + np.arange(bs)[None, :]).ravel()
+        x = torch.full((p.n_local * bs,), float("nan"), dtype=torch.float64, device="cuda")
+        x[:p.n_own * bs] = torch.from_numpy(want[:p.n_own * bs]).cuda()
+        send = torch.empty(p.n_send * bs, dtype=torch.float64, device="cuda")
+        p.pack_blocks(x.data_ptr(), bs, send.data_ptr(), 0)
+        xs.append((x, want))
+        sends.append(send)
+    for p, (x, want) in zip(plans, xs):
+        recv = torch.empty(p.n_recv * bs, dtype=torch.float64, device="cuda")
+        for k, q in enumerate(p.nb_ranks):
+            pq = plans[q]
+            kk = int(np.where(pq.nb_ranks == p.rank)[0][0])
+            recv[p.recv_offsets[k] * bs:p.recv_offsets[k + 1] * bs] = \
+                sends[q][pq.send_offsets[kk] * bs:pq.send_offsets[kk + 1] * bs]
+        p.unpack_blocks(recv.data_ptr(), bs, x.data_ptr(), 0)
+        torch.cuda.synchronize()
+        assert np.array_equal(x.cpu().numpy(), want)

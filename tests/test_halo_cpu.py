@@ -86,17 +86,29 @@ def test_plan_arguments_are_checked(cb):
     assert one.n_own == one.n_local == mesh.n_cells and one.nb_ranks.size == 0
 
 
-def _numpy_packer(plan):
-    """pack_soa_to_aos / unpack_aos_to_soa (src/fields/halo.cpp:26-124) in numpy."""
-    def pack(fields, send):
-        a = np.stack([f.numpy()[plan.send_owned_local] for f in fields], axis=1)
-        send.copy_(__import__("torch").from_numpy(a.ravel()))
+class _NumpyPacker:
+    """pack_soa_to_aos / unpack_aos_to_soa (src/fields/halo.cpp:26-124) and
+    the vector layout's block packing (vector_layout.hpp:172-260) in numpy."""
 
-    def unpack(recv, fields):
+    def __init__(self, plan):
+        self.plan = plan
+
+    def pack(self, fields, send):
+        import torch
+        a = np.stack([f.numpy()[self.plan.send_owned_local] for f in fields], axis=1)
+        send.copy_(torch.from_numpy(a.ravel()))
+
+    def unpack(self, recv, fields):
         a = recv.numpy().reshape(-1, len(fields))
         for v, f in enumerate(fields):
-            f.numpy()[plan.recv_ghost_local] = a[:, v]
-    return pack, unpack
+            f.numpy()[self.plan.recv_ghost_local] = a[:, v]
+
+    def pack_blocks(self, x, bs, send):
+        import torch
+        send.copy_(torch.from_numpy(x.numpy().reshape(-1, bs)[self.plan.send_owned_local].ravel()))
+
+    def unpack_blocks(self, recv, bs, x):
+        x.numpy().reshape(-1, bs)[self.plan.recv_ghost_local] = recv.numpy().reshape(-1, bs)
 
 
 def _free_port():
@@ -127,7 +139,7 @@ def _rank(rank, world, port, out_dir):
             return f
         rho, e = field(2.0), field(-3.0)
         gx, gy, gz, phi = field(5.0), field(7.0), field(11.0), field(0.5)
-        ex = cb.halo.HaloExchanger(plan, packer=_numpy_packer(plan))
+        ex = cb.halo.HaloExchanger(plan, packer=_NumpyPacker(plan))
         ex.register_cell_fields([rho, e])
         ex.register_grad_limiters([gx], [gy], [gz], [phi])
         ex.start_exchange_fields()
@@ -138,6 +150,12 @@ def _rank(rank, world, port, out_dir):
         ok = True
         for f, s in ((rho, 2.0), (e, -3.0), (gx, 5.0), (gy, 7.0), (gz, 11.0), (phi, 0.5), (once, 13.0)):
             ok = ok and np.array_equal(f.numpy(), s * g + 1.0)
+        # a Krylov-layout block vector (6 entries a row)
+        xv = torch.full((plan.n_local * 6,), float("nan"), dtype=torch.float64)
+        want = (g[:, None] * 10.0 + np.arange(6)[None, :]).ravel()
+        xv[:plan.n_own * 6] = torch.from_numpy(want[:plan.n_own * 6])
+        ex.exchange_vector(xv, 6)
+        ok = ok and np.array_equal(xv.numpy(), want)
         total = cb.halo.allreduce_sum(torch.tensor([float(plan.n_own)], dtype=torch.float64))
         Path(out_dir, f"r{rank}.txt").write_text(
             f"{int(ok)} {ex.num_registered_fields} {ex.num_registered_grads_and_limiters} {int(total.item())}")
