@@ -163,36 +163,70 @@ private:
 // BiCGSTAB on the device (right-preconditioned, the reference's recurrences,
 // scalars and inner products on the device): A a GpuBsrOperator, M a GpuSgs
 // set up on it or an IdentityPreconditioner; x holds the initial guess.
+// The operator and preconditioner checks of the GPU Krylov solvers: a
+// GpuBsrOperator, and GpuSgs set up on it or the identity.
+inline int gpu_krylov_precond(const linalg::LinearOperator& A, const linalg::Preconditioner& M, const char* who,
+                              const GpuBsrOperator*& op) {
+    const MPI_Comm comm = A.layout().comm();
+    op = dynamic_cast<const GpuBsrOperator*>(&A);
+    linalg::check(op != nullptr, comm, std::string(who) + ": the operator must be a GpuBsrOperator");
+    if (const auto* sgs = dynamic_cast<const GpuSgs*>(&M)) {
+        linalg::check(sgs->op() == op, comm, std::string(who) + ": the GpuSgs was set up on another operator");
+        return CFDG_PC_SGS;
+    }
+    linalg::check(dynamic_cast<const linalg::IdentityPreconditioner*>(&M) != nullptr, comm,
+                  std::string(who) + ": GpuSgs or IdentityPreconditioner");
+    return CFDG_PC_NONE;
+}
+
+inline linalg::IterationResult gpu_krylov_result(const cfdg_krylov_result& r) {
+    linalg::IterationResult out;
+    out.status = r.status == CFDG_KRYLOV_CONVERGED   ? linalg::SolverStatus::Converged
+                 : r.status == CFDG_KRYLOV_DIVERGED ? linalg::SolverStatus::Diverged
+                                                     : linalg::SolverStatus::MaxIterations;
+    out.iterations = r.iterations;
+    out.initial_residual = r.initial_residual;
+    out.final_residual = r.final_residual;
+    return out;
+}
+
 class GpuBiCGSTAB final : public linalg::IterativeSolver {
 public:
     const char* name() const override { return "BiCGSTAB (cfdg, GPU)"; }
     linalg::IterationResult solve(const linalg::LinearOperator& A, const linalg::Preconditioner& M,
                                   linalg::Vector& x, const linalg::Vector& b) override {
-        const MPI_Comm comm = A.layout().comm();
-        const auto* op = dynamic_cast<const GpuBsrOperator*>(&A);
-        linalg::check(op != nullptr, comm, "GpuBiCGSTAB: the operator must be a GpuBsrOperator");
-        int precond = CFDG_PC_NONE;
-        if (const auto* sgs = dynamic_cast<const GpuSgs*>(&M)) {
-            linalg::check(sgs->op() == op, comm, "GpuBiCGSTAB: the GpuSgs was set up on another operator");
-            precond = CFDG_PC_SGS;
-        } else {
-            linalg::check(dynamic_cast<const linalg::IdentityPreconditioner*>(&M) != nullptr, comm,
-                          "GpuBiCGSTAB: GpuSgs or IdentityPreconditioner");
-        }
+        const GpuBsrOperator* op = nullptr;
+        const int precond = gpu_krylov_precond(A, M, "GpuBiCGSTAB", op);
         cfdg_krylov_result r{};
         require(cfdg_bicgstab_host(op->handle(), precond, params_.relative_tolerance, params_.absolute_tolerance,
                                    params_.max_iterations, x.data(), b.data(), &r),
-                comm, "GpuBiCGSTAB::solve");
-        linalg::IterationResult out;
-        out.status = r.status == CFDG_KRYLOV_CONVERGED   ? linalg::SolverStatus::Converged
-                     : r.status == CFDG_KRYLOV_DIVERGED ? linalg::SolverStatus::Diverged
-                                                         : linalg::SolverStatus::MaxIterations;
-        out.iterations = r.iterations;
-        out.initial_residual = r.initial_residual;
-        out.final_residual = r.final_residual;
-        last_ = out;
-        return out;
+                A.layout().comm(), "GpuBiCGSTAB::solve");
+        last_ = gpu_krylov_result(r);
+        return last_;
     }
+};
+
+// Restarted GMRES(restart) with right preconditioning behind the same
+// IterativeSolver interface (not in the reference: the Krylov method of the
+// library's Jacobian-free solves, offered here for any operator).
+class GpuGmres final : public linalg::IterativeSolver {
+public:
+    explicit GpuGmres(int restart = 30) : restart_(restart) {}
+    const char* name() const override { return "GMRES (cfdg, GPU)"; }
+    linalg::IterationResult solve(const linalg::LinearOperator& A, const linalg::Preconditioner& M,
+                                  linalg::Vector& x, const linalg::Vector& b) override {
+        const GpuBsrOperator* op = nullptr;
+        const int precond = gpu_krylov_precond(A, M, "GpuGmres", op);
+        cfdg_krylov_result r{};
+        require(cfdg_gmres_host(op->handle(), precond, params_.relative_tolerance, params_.absolute_tolerance,
+                                params_.max_iterations, restart_, x.data(), b.data(), &r),
+                A.layout().comm(), "GpuGmres::solve");
+        last_ = gpu_krylov_result(r);
+        return last_;
+    }
+
+private:
+    int restart_;
 };
 
 // ------------------------------------------------------------- gradient

@@ -94,7 +94,8 @@ void run_solver(const cfdg_mesh_host& m, const cfdg_config& c, const cfdg_bc_des
 // mode 0: reference BiCGSTAB, reference BsrMatrix, reference SgsPreconditioner;
 // mode 1: reference BiCGSTAB and BsrMatrix, GpuSgs (level sweep) set up on the BsrMatrix;
 // mode 2: reference BiCGSTAB, GpuBsrOperator, GpuSgs;
-// mode 3: GpuBiCGSTAB, GpuBsrOperator, GpuSgs.
+// mode 3: GpuBiCGSTAB, GpuBsrOperator, GpuSgs;
+// mode 4: GpuGmres(30), GpuBsrOperator, GpuSgs.
 RB_API int rb_bicgstab(int n, int bs, const int32_t* row_ptr, const int32_t* cols, const double* vals,
                        const double* b, double* x, int mode, double rtol, int max_it, int* iterations, int* status,
                        double* final_residual) {
@@ -106,6 +107,7 @@ RB_API int rb_bicgstab(int n, int bs, const int32_t* row_ptr, const int32_t* col
     if (mode == 0) M = std::make_unique<linalg::SgsPreconditioner>();
     else M = std::make_unique<rb::GpuSgs>(CFDG_SGS_LEVEL);
     if (mode == 3) K = std::make_unique<rb::GpuBiCGSTAB>();
+    else if (mode == 4) K = std::make_unique<rb::GpuGmres>(30);
     else K = std::make_unique<linalg::BiCGSTAB>();
     const linalg::LinearOperator& op = G ? static_cast<const linalg::LinearOperator&>(*G) : *A;
     M->setup(op);

@@ -53,6 +53,16 @@ def test_reference_krylov_with_gpu_adapters(refbind, ramp_system, mode):
     assert rel_err(x, x_ref) < 1e-8
 
 
+def test_gpu_gmres_behind_the_iterative_solver_interface(refbind, ramp_system):
+    """GpuGmres through linalg::IterativeSolver (GpuBsrOperator, GpuSgs):
+    the reference BiCGSTAB's solution of the same tightly solved system."""
+    row_ptr, cols, vals, b = ramp_system
+    x_ref, r_ref = refbind.bicgstab(row_ptr, cols, vals, 5, b, 0, rel_tol=1e-10, max_it=200)
+    x, r = refbind.bicgstab(row_ptr, cols, vals, 5, b, 4, rel_tol=1e-10, max_it=400)
+    assert r_ref["status"] == 0 and r["status"] == 0
+    assert rel_err(x, x_ref) < 1e-8
+
+
 @pytest.mark.parametrize("stencil", [2, 3], ids=["face", "node"])
 def test_gpu_gradient_operator(cb, refbind, stencil):
     case = cb.cases.plate(scale=8)
